@@ -1,0 +1,1125 @@
+// build.cu -- the spatial rebuild of one Barnes-Hut step on sm_100a.
+//
+// Stage map (reference file:line each kernel replaces, paths relative to the
+// sytrams/AMSC-Nbody project root):
+//   kd_bbox_kernel        integrator.cu:57-89 (KD) fused with
+//                         globalbounding.cu:130-180 (Bbox)
+//   encode_kernel         morton.cu:147-188 (normalise/quantise/interleave)
+//                         + the digit histograms of the radix sort
+//   onesweep_kernel       morton.cu:270-273 (stable_sort_by_key), in-house
+//                         LSD radix sort with decoupled look-back
+//   groups_kernel         morton_leaf_groups.cu:105-150 (RLE + scan) fused
+//                         with simulation.cu:34-58 (Morton-order gather)
+//   karras_kernel         tree_builder.cu:9-113
+//   plan_kernel           radix_to_octree.cu:140-215 + its exclusive scan
+//   octree_clear_kernel   octree_builder.cu:476-509 (initialisation)
+//   materialize_kernel    octree_builder.cu:275-412
+//   node_init_kernel      octree_geometry.cu:56-102 + octree_physics.cu:236-326
+//   propagate_kernel      octree_physics.cu:328-417 (+ subtree sizes)
+//   layout_kernel         traversal records in depth-first preorder
+//
+// No kernel synchronises with the host: data-dependent sizes (G, M) live in
+// device memory and every later kernel bounds its grid-stride loop by them.
+#include "nbb_internal.cuh"
+
+#include <cfloat>
+#include <cmath>
+
+namespace nbb {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+inline int grid_for(const Workspace &ws, int per_sm = 8) {
+  return ws.num_sms > 0 ? ws.num_sms * per_sm : 1184;
+}
+
+// ------------------------------------------------------------- reset ----
+
+__global__ void reset_scalars_kernel(DevScalars *sc) {
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < 3; ++a) {
+      sc->bb_min[a] = ~0ull;
+      sc->bb_max[a] = 0ull;
+    }
+    sc->nonfinite = 0;
+    sc->n_groups = 0;
+    sc->n_nodes = 0;
+    sc->ticket_bbox = 0;
+    sc->ticket_encode = 0;
+    for (int k = 0; k < 8; ++k) sc->tile_counter[k] = 0;
+    sc->work_counter = 0;
+    sc->stack_overflow = 0;
+    sc->interactions = 0;
+    sc->mac_tests = 0;
+  }
+}
+
+// --------------------------------------------------------- KD + bbox ----
+
+template <typename T>
+__device__ __forceinline__ T warp_reduce_min(T v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_reduce_max(T v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One pass over the state: optional first half kick + drift
+// (integrator.cu:57-89), then the extrema of the new positions and a
+// non-finite flag (globalbounding.cu:62-92).  The last block to finish forms
+// centre = (min + max) * 0.5 and side = 1.1 * longest extent, or 1 when that
+// is 0 (globalbounding.cu:158-172).
+__global__ void __launch_bounds__(kBlock) kd_bbox_kernel(Workspace ws, double dt,
+                                                         int do_kd) {
+  __shared__ double s_lo[3][kBlock / 32], s_hi[3][kBlock / 32];
+  __shared__ int s_nf[kBlock / 32];
+  __shared__ bool s_last;
+  const int n = ws.n;
+  const double hdt = 0.5 * dt;
+  double lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY;
+  double hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
+  int nf = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double px = ws.x[i], py = ws.y[i], pz = ws.z[i];
+    if (do_kd) {
+      const double vx = __fma_rn(hdt, ws.ax[i], ws.vx[i]);
+      const double vy = __fma_rn(hdt, ws.ay[i], ws.vy[i]);
+      const double vz = __fma_rn(hdt, ws.az[i], ws.vz[i]);
+      ws.vx[i] = vx;
+      ws.vy[i] = vy;
+      ws.vz[i] = vz;
+      px = __fma_rn(dt, vx, px);
+      py = __fma_rn(dt, vy, py);
+      pz = __fma_rn(dt, vz, pz);
+      ws.x[i] = px;
+      ws.y[i] = py;
+      ws.z[i] = pz;
+    }
+    nf |= !(isfinite(px) && isfinite(py) && isfinite(pz));
+    lo0 = fmin(lo0, px); hi0 = fmax(hi0, px);
+    lo1 = fmin(lo1, py); hi1 = fmax(hi1, py);
+    lo2 = fmin(lo2, pz); hi2 = fmax(hi2, pz);
+  }
+  lo0 = warp_reduce_min(lo0); lo1 = warp_reduce_min(lo1); lo2 = warp_reduce_min(lo2);
+  hi0 = warp_reduce_max(hi0); hi1 = warp_reduce_max(hi1); hi2 = warp_reduce_max(hi2);
+  nf = __any_sync(0xffffffffu, nf);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    s_lo[0][warp] = lo0; s_lo[1][warp] = lo1; s_lo[2][warp] = lo2;
+    s_hi[0][warp] = hi0; s_hi[1][warp] = hi1; s_hi[2][warp] = hi2;
+    s_nf[warp] = nf;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    DevScalars *sc = ws.sc;
+    int anynf = 0;
+    for (int a = 0; a < 3; ++a) {
+      double lo = INFINITY, hi = -INFINITY;
+      for (int w = 0; w < kBlock / 32; ++w) {
+        lo = fmin(lo, s_lo[a][w]);
+        hi = fmax(hi, s_hi[a][w]);
+      }
+      if (lo <= hi) {
+        atomicMin(&sc->bb_min[a], order_bits(lo));
+        atomicMax(&sc->bb_max[a], order_bits(hi));
+      }
+    }
+    for (int w = 0; w < kBlock / 32; ++w) anynf |= s_nf[w];
+    if (anynf) atomicOr(&sc->nonfinite, 1);
+    __threadfence();
+    const unsigned t = atomicAdd(&sc->ticket_bbox, 1u);
+    s_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    DevScalars *sc = ws.sc;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = order_value(atomicAdd(&sc->bb_min[a], 0ull));
+      hi[a] = order_value(atomicAdd(&sc->bb_max[a], 0ull));
+    }
+    const int bad = atomicAdd(&sc->nonfinite, 0);
+    if (bad) record_error(sc, kStageBbox, 1);
+    for (int a = 0; a < 3; ++a) sc->box[a] = __dmul_rn(__dadd_rn(lo[a], hi[a]), 0.5);
+    double ext = __dsub_rn(hi[0], lo[0]);
+    const double ey = __dsub_rn(hi[1], lo[1]);
+    const double ez = __dsub_rn(hi[2], lo[2]);
+    if (ey > ext) ext = ey;
+    if (ez > ext) ext = ez;
+    double side = __dmul_rn(1.1, ext);
+    if (side == 0.0) side = 1.0;
+    sc->box[3] = side;
+  }
+}
+
+// ---------------------------------------------------- Morton encode ----
+
+// morton.cu:168-177
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+  uint32_t x = v & 0x000003FFu;
+  x = (x | (x << 16)) & 0x030000FFu;
+  x = (x | (x << 8)) & 0x0300F00Fu;
+  x = (x | (x << 4)) & 0x030C30C3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// morton.cu:147-166 with explicitly rounded operations: the normalised
+// coordinate is a true division, then scaled by the 1024-cell grid, clamped
+// to [0, 1023] and truncated.
+__device__ __forceinline__ uint32_t quantise(double a, double lower, double side) {
+  const double normalised = __ddiv_rn(__dsub_rn(a, lower), side);
+  const double scaled = __dmul_rn(normalised, 1024.0);
+  const double clamped = fmin(fmax(scaled, 0.0), 1023.0);
+  return (uint32_t)clamped;
+}
+
+// Keys and packed (key << 32 | index) pairs, plus the 4 x 256 digit
+// histograms of the sort passes; the last block turns the histograms into
+// exclusive digit offsets.
+__global__ void __launch_bounds__(kBlock) encode_kernel(Workspace ws) {
+  __shared__ uint32_t hist[kSortPasses][256];
+  __shared__ bool s_last;
+  for (int k = threadIdx.x; k < kSortPasses * 256; k += blockDim.x) (&hist[0][0])[k] = 0;
+  __syncthreads();
+  DevScalars *sc = ws.sc;
+  const double cxx = sc->box[0], cyy = sc->box[1], czz = sc->box[2], side = sc->box[3];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // morton.cu:218-219
+    if (!isfinite(cxx) || !isfinite(cyy) || !isfinite(czz) || !isfinite(side) || side <= 0.0)
+      record_error(sc, kStageBbox, 2);
+  }
+  const double half_side = __dmul_rn(side, 0.5);  // side / 2.0, exact
+  const double lx = __dsub_rn(cxx, half_side);
+  const double ly = __dsub_rn(cyy, half_side);
+  const double lz = __dsub_rn(czz, half_side);
+  const int n = ws.n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t qx = quantise(ws.x[i], lx, side);
+    const uint32_t qy = quantise(ws.y[i], ly, side);
+    const uint32_t qz = quantise(ws.z[i], lz, side);
+    const uint32_t key = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
+    ws.pairs_a[i] = ((unsigned long long)key << 32) | (unsigned)i;
+#pragma unroll
+    for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (8 * p)) & 255u], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kSortPasses * 256; k += blockDim.x) {
+    const uint32_t c = (&hist[0][0])[k];
+    if (c) atomicAdd(&ws.digit_hist[k], c);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&sc->ticket_encode, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    if (threadIdx.x < kSortPasses) {
+      uint32_t *h = ws.digit_hist + threadIdx.x * 256;
+      uint32_t run = 0;
+      for (int d = 0; d < 256; ++d) {
+        const uint32_t c = atomicAdd(&h[d], 0u);
+        h[d] = run;
+        run += c;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------ onesweep pass ----
+
+constexpr uint32_t kDigitFlagA = 1u << 30;  // tile aggregate published
+constexpr uint32_t kDigitFlagP = 2u << 30;  // inclusive prefix published
+constexpr uint32_t kDigitMask = (1u << 30) - 1u;
+
+// One stable LSD pass over 8 key bits.  A tile's items are ranked warp by
+// warp and round by round in input order (match_any groups equal digits in a
+// round), so equal digits keep their input order: the result is the stable
+// order of thrust::stable_sort_by_key.  Tile prefixes per digit come from a
+// decoupled look-back over the tiles launched before it (tile ids are taken
+// from an atomic counter, so every predecessor is already running).
+__global__ void __launch_bounds__(kSortThreads)
+    onesweep_kernel(const unsigned long long *__restrict__ in,
+                    unsigned long long *__restrict__ out, int n, int pass,
+                    const uint32_t *__restrict__ digit_offsets,
+                    uint32_t *status, DevScalars *sc) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t whist[kWarps][256];
+  __shared__ uint32_t digit_base[256];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) s_tile = (int)atomicAdd(&sc->tile_counter[pass], 1u);
+  for (int k = tid; k < kWarps * 256; k += kSortThreads) (&whist[0][0])[k] = 0;
+  __syncthreads();
+  const int tile = s_tile;
+  const int shift = 32 + 8 * pass;
+  const int start = tile * kSortTile + warp * (32 * kSortItems);
+  unsigned long long key[kSortItems];
+  uint32_t rank[kSortItems];
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const int i = start + it * 32 + lane;
+    key[it] = (i < n) ? in[i] : ~0ull;
+  }
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const int i = start + it * 32 + lane;
+    const bool valid = i < n;
+    const uint32_t dig = (uint32_t)(key[it] >> shift) & 255u;
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? dig : 0xFFFFFFFFu);
+    uint32_t base = 0;
+    if (valid) base = whist[warp][dig];
+    __syncwarp();
+    if (valid) {
+      rank[it] = base + __popc(peers & lt);
+      if ((peers & lt) == 0) whist[warp][dig] = base + __popc(peers);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  if (tid < 256) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = whist[w][tid];
+      whist[w][tid] = run;
+      run += c;
+    }
+    uint32_t *my = status + (size_t)tile * 256 + tid;
+    uint32_t prefix = 0;
+    if (tile == 0) {
+      st_release_u32(my, kDigitFlagP | run);
+    } else {
+      st_release_u32(my, kDigitFlagA | run);
+      int j = tile - 1;
+      int spins = 0;
+      while (j >= 0) {
+        const uint32_t s = ld_acquire_u32(status + (size_t)j * 256 + tid);
+        const uint32_t flag = s & ~kDigitMask;
+        if (flag == 0u) {
+          if (++spins > kSpinLimit) {
+            record_error(sc, kStageSort, kCodeTimeout);
+            break;
+          }
+          continue;
+        }
+        prefix += s & kDigitMask;
+        if (flag == kDigitFlagP) break;
+        --j;
+      }
+      st_release_u32(my, kDigitFlagP | (prefix + run));
+    }
+    digit_base[tid] = digit_offsets[pass * 256 + tid] + prefix;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < kSortItems; ++it) {
+    const int i = start + it * 32 + lane;
+    if (i < n) {
+      const uint32_t dig = (uint32_t)(key[it] >> shift) & 255u;
+      const uint32_t pos = digit_base[dig] + whist[warp][dig] + rank[it];
+      if (pos < (uint32_t)n) {
+        out[pos] = key[it];
+      } else {
+        record_error(sc, kStageSort, 1);
+      }
+    }
+  }
+}
+
+// ------------------------------------------- single-pass scan helpers ----
+
+constexpr unsigned long long kScanFlagA = 1ull << 62;
+constexpr unsigned long long kScanFlagP = 2ull << 62;
+constexpr unsigned long long kScanMask = (1ull << 62) - 1ull;
+
+// Decoupled look-back by one full warp: publishes this tile's aggregate,
+// accumulates predecessors until one with an inclusive prefix, publishes the
+// inclusive prefix and returns the exclusive one.
+__device__ unsigned long long warp_lookback(unsigned long long *status, int tile,
+                                            unsigned long long aggregate,
+                                            DevScalars *sc, int stage) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_release_u64(status, kScanFlagP | aggregate);
+    return 0ull;
+  }
+  if (lane == 0) st_release_u64(status + tile, kScanFlagA | aggregate);
+  unsigned long long excl = 0;
+  int j = tile - 1;
+  while (true) {
+    const int idx = j - lane;
+    unsigned long long s = kScanFlagP;
+    if (idx >= 0) {
+      s = ld_acquire_u64(status + idx);
+      int spins = 0;
+      while ((s >> 62) == 0ull) {
+        if (++spins > kSpinLimit) {
+          record_error(sc, stage, kCodeTimeout);
+          s = kScanFlagP;
+          break;
+        }
+        s = ld_acquire_u64(status + idx);
+      }
+    }
+    const unsigned pmask = __ballot_sync(0xffffffffu, (s >> 62) == 2ull);
+    unsigned long long v = s & kScanMask;
+    if (pmask) {
+      const int stop = __ffs(pmask) - 1;
+      if (lane > stop) v = 0;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      excl += v;
+      break;
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    j -= 32;
+  }
+  if (lane == 0) st_release_u64(status + tile, kScanFlagP | (excl + aggregate));
+  return excl;
+}
+
+// Block-wide exclusive scan of ITEMS rows of 0/1 or small int values laid
+// out row-major (element (k, tid) precedes (k, tid+1) and (k+1, 0)).  Each
+// thread passes its values; returns per-row exclusive offsets in `excl` and
+// the block total.  `row_warp` is shared scratch of ITEMS * warps ints.
+template <int ITEMS, int THREADS>
+__device__ unsigned long long block_scan_rows(const int (&val)[ITEMS], int (&excl)[ITEMS],
+                                              unsigned long long *row_warp,
+                                              unsigned long long *s_total) {
+  constexpr int kWarps = THREADS / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    int v = val[k];
+    // warp inclusive scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += t;
+    }
+    excl[k] = v - val[k];
+    if (lane == 31) row_warp[k * kWarps + warp] = (unsigned long long)v;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int kCount = ITEMS * kWarps;
+    static_assert(kCount % 32 == 0, "scan rows must fill whole warps");
+    unsigned long long carry = 0;
+    for (int base = 0; base < kCount; base += 32) {
+      unsigned long long v = row_warp[base + lane];
+      unsigned long long inc = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      row_warp[base + lane] = carry + inc - v;
+      carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0) *s_total = carry;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) excl[k] += (int)row_warp[k * kWarps + warp];
+  return *s_total;
+}
+
+// ------------------------------------------------------------ groups ----
+
+// Run-length encoding of the sorted keys as a scan of "key differs from its
+// predecessor" flags: a group starts where the flag is set; its id is the
+// number of flags before it.  Also splits the packed pairs into the
+// reference's key / index arrays and gathers {x, y, z, m} into Morton order.
+__global__ void __launch_bounds__(kScanThreads) groups_kernel(Workspace ws,
+                                                              int gather) {
+  __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
+  __shared__ unsigned long long s_total, s_prefix;
+  __shared__ int s_tile;
+  DevScalars *sc = ws.sc;
+  const int n = ws.n;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[4], 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  const int base = tile * kScanTile;
+  if (base >= n) return;
+  const unsigned long long *pairs = ws.pairs_a;
+  int flag[kScanItems], excl[kScanItems];
+  uint32_t key[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    flag[k] = 0;
+    key[k] = 0;
+    if (i < n) {
+      key[k] = (uint32_t)(pairs[i] >> 32);
+      flag[k] = (i == 0) || (key[k] != (uint32_t)(pairs[i - 1] >> 32));
+    }
+  }
+  const unsigned long long total = block_scan_rows<kScanItems, kScanThreads>(flag, excl, row_warp, &s_total);
+  if (threadIdx.x < 32) {
+    const unsigned long long p = warp_lookback(ws.scan_status, tile, total, sc, kStageGroups);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  const int prefix = (int)s_prefix;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    if (i >= n) continue;
+    const int g = prefix + excl[k] + flag[k] - 1;
+    const unsigned long long pr = pairs[i];
+    const uint32_t id = (uint32_t)(pr & 0xffffffffu);
+    if (g < 0 || g >= n || id >= (uint32_t)n) {
+      record_error(sc, kStageGroups, 1);
+      continue;
+    }
+    if (flag[k]) {
+      ws.uniq[g] = key[k];
+      ws.gfirst[g] = i;
+    }
+    const bool last = (i == n - 1) || ((uint32_t)(pairs[i + 1] >> 32) != key[k]);
+    if (last) ws.glast[g] = i;
+    ws.keys[i] = key[k];
+    ws.idx[i] = id;
+    if (gather) ws.pm4[i] = make_double4(ws.x[id], ws.y[id], ws.z[id], ws.m[id]);
+  }
+  if (base + kScanTile >= n && threadIdx.x == 0) sc->n_groups = prefix + (int)total;
+}
+
+// ------------------------------------------------------------ Karras ----
+
+// tree_builder.cu:9-24
+__device__ __forceinline__ int lcp(const uint32_t *keys, int i, int j, int n) {
+  if (j < 0 || j >= n) return -1;
+  if (i == j) return 64;
+  const uint32_t a = keys[i], b = keys[j];
+  if (a != b) return __clz(a ^ b);
+  return 32 + __clz((uint32_t)(i ^ j));
+}
+
+// tree_builder.cu:30-113 for internal node i of a tree over n keys.
+__device__ void karras_node(const uint32_t *keys, int n, int i, int *left, int *right,
+                            int *rfirst, int *rlast, int *plen, int *parent) {
+  const int dright = lcp(keys, i, i + 1, n);
+  const int dleft = lcp(keys, i, i - 1, n);
+  const int dir = (dright > dleft) ? 1 : -1;
+  const int dmin = lcp(keys, i, i - dir, n);
+  int length = 2;
+  while (lcp(keys, i, i + length * dir, n) > dmin) length *= 2;
+  int l = 0;
+  for (int t = length / 2; t >= 1; t /= 2)
+    if (lcp(keys, i, i + (l + t) * dir, n) > dmin) l += t;
+  const int j = i + l * dir;
+  const int first = (i < j) ? i : j;
+  const int last = (i > j) ? i : j;
+  rfirst[i] = first;
+  rlast[i] = last;
+  const int node_prefix = lcp(keys, first, last, n);
+  plen[i] = node_prefix;
+  // findSplit (tree_builder.cu:64-84), including the candidate < last guard
+  int split = first;
+  if (first < last) {
+    int step = last - first;
+    do {
+      step = (step + 1) >> 1;
+      const int candidate = split + step;
+      if (candidate < last && lcp(keys, first, candidate, n) > node_prefix) split = candidate;
+    } while (step > 1);
+  }
+  const int lc = (split == first) ? split : n + split;
+  const int rc = (split + 1 == last) ? split + 1 : n + split + 1;
+  left[i] = lc;
+  right[i] = rc;
+  parent[lc] = n + i;
+  parent[rc] = n + i;
+}
+
+// Karras tree over the G unique keys; also finishes the group counts.  The
+// root (internal node 0, id G) keeps parent -1; every other node's parent is
+// written by exactly one thread, which equals the reference's memset + write.
+__global__ void __launch_bounds__(kBlock) karras_kernel(Workspace ws) {
+  if (ws.sc->error) return;
+  const int g = ws.sc->n_groups;
+  if (g <= 0 || g > ws.n) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) record_error(ws.sc, kStageGroups, 2);
+    return;
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x) {
+    ws.gcount[i] = ws.glast[i] - ws.gfirst[i] + 1;
+    if (i == 0) ws.rparent[g == 1 ? 0 : g] = -1;
+    if (i < g - 1)
+      karras_node(ws.uniq, g, i, ws.left, ws.right, ws.rfirst, ws.rlast, ws.plen, ws.rparent);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+    karras_only_kernel(const uint32_t *keys, int n, int *left, int *right, int *rfirst,
+                       int *rlast, int *plen, int *parent) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i == 0) parent[n == 1 ? 0 : n] = -1;
+    if (i < n - 1) karras_node(keys, n, i, left, right, rfirst, rlast, plen, parent);
+  }
+}
+
+// -------------------------------------------------------------- plan ----
+
+// radix_to_octree.cu:124-138
+__device__ __forceinline__ int octree_level_of(int n_leaves, const int *plen, int r) {
+  const int prefix = (r < n_leaves) ? kSpatialBits : plen[r - n_leaves] - kPaddingBits;
+  return prefix / kDims;
+}
+
+// radix_to_octree.cu:140-215 for radix node r; returns the edge node count.
+__device__ int plan_node(const Workspace &ws, int g, int r) {
+  const int nr = 2 * g - 1;
+  DevScalars *sc = ws.sc;
+  auto fail = [&](int code) {
+    record_error(sc, kStagePlan, code);
+    ws.plevel[r] = 0;
+    ws.pcount[r] = 0;
+    return 0;
+  };
+  if (r < g) {
+    if ((ws.uniq[r] & ~kSpatialMask) != 0u) return fail(1);
+  } else {
+    const int sp = ws.plen[r - g] - kPaddingBits;
+    if (sp < 0 || sp >= kSpatialBits) return fail(4);
+  }
+  const int p = ws.rparent[r];
+  int parent_level = 0;
+  if (p != -1) {
+    if (p < g || p >= nr) return fail(2);
+    parent_level = octree_level_of(g, ws.plen, p);
+  }
+  const int node_level = (r < g) ? parent_level + 1 : octree_level_of(g, ws.plen, r);
+  if (node_level < 0 || node_level > kMaxLevel) return fail(3);
+  if (node_level < parent_level) return fail(3);
+  ws.plevel[r] = node_level;
+  ws.pcount[r] = node_level - parent_level;
+  return node_level - parent_level;
+}
+
+// Plan values + their exclusive scan in one pass; the last tile sets
+// M = 1 + sum (radix_to_octree.cu:291-313), bounded by the node capacity.
+__global__ void __launch_bounds__(kScanThreads) plan_kernel(Workspace ws) {
+  __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
+  __shared__ unsigned long long s_total, s_prefix;
+  __shared__ int s_tile;
+  DevScalars *sc = ws.sc;
+  const int g = sc->n_groups;
+  if (g <= 0 || g > ws.n || sc->error) return;
+  const int nr = 2 * g - 1;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[5], 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  const int base = tile * kScanTile;
+  if (base >= nr) return;
+  int val[kScanItems], excl[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int r = base + k * kScanThreads + threadIdx.x;
+    val[k] = (r < nr) ? plan_node(ws, g, r) : 0;
+  }
+  const unsigned long long total = block_scan_rows<kScanItems, kScanThreads>(val, excl, row_warp, &s_total);
+  if (threadIdx.x < 32) {
+    const unsigned long long p =
+        warp_lookback(ws.scan_status + ws.scan_tiles_n, tile, total, sc, kStagePlan);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  const long long prefix = (long long)s_prefix;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int r = base + k * kScanThreads + threadIdx.x;
+    if (r < nr) ws.poffset[r] = (int)(prefix + excl[k]);
+  }
+  if (base + kScanTile >= nr && threadIdx.x == 0) {
+    const long long m = 1 + prefix + (long long)total;
+    if (m > ws.cap_nodes) {
+      record_error(sc, kStagePlan, kCodeOverflow);
+      sc->n_nodes = 0;
+    } else {
+      sc->n_nodes = (int)m;
+    }
+  }
+}
+
+// ------------------------------------------------------------ octree ----
+
+// octree_builder.cu:476-509: empty child slots and parents -1, root level 0.
+__global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
+  const int m = ws.sc->n_nodes;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+    int4 *c = reinterpret_cast<int4 *>(ws.children + (size_t)i * 8);
+    c[0] = make_int4(-1, -1, -1, -1);
+    c[1] = make_int4(-1, -1, -1, -1);
+    ws.oparent[i] = -1;
+    ws.olevel[i] = (i == 0) ? 0 : -1;
+    ws.oprefix[i] = 0u;
+    ws.ofirst[i] = -1;
+    ws.ocount[i] = 0;
+    ws.pending[i] = 0;
+    ws.child_count[i] = 0;
+    ws.subtree[i] = 0;
+    ws.preoff[i] = 0;
+    ws.mass[i] = 0.0;
+    ws.comx[i] = 0.0;
+    ws.comy[i] = 0.0;
+    ws.comz[i] = 0.0;
+  }
+}
+
+// octree_builder.cu:237-254
+__device__ __forceinline__ uint32_t prefix_at_level(uint32_t key, int level) {
+  if (level == 0) return 0u;
+  const int rem = kSpatialBits - level * kDims;
+  return key & (kSpatialMask & (~0u << rem));
+}
+__device__ __forceinline__ int octant_at_level(uint32_t key, int level) {
+  return (int)((key >> (kSpatialBits - level * kDims)) & 7u);
+}
+
+// octree_builder.cu:275-412: each radix edge emits its chain of octree nodes
+// at ids 1 + edgeNodeOffset[r] + k; children slots are claimed with
+// atomicCAS so a collision is detected as the reference does.
+__global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
+  DevScalars *sc = ws.sc;
+  const int g = sc->n_groups;
+  const int m = sc->n_nodes;
+  if (g <= 0 || g > ws.n || m <= 0 || sc->error) return;
+  const int nr = 2 * g - 1;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += gridDim.x * blockDim.x) {
+    const int count = ws.pcount[r];
+    const int node_level = ws.plevel[r];
+    if (count < 0 || node_level < 0 || node_level > kMaxLevel) {
+      record_error(sc, kStageOctree, 1);
+      continue;
+    }
+    if (count == 0) {
+      if (r < g) record_error(sc, kStageOctree, 5);
+      continue;
+    }
+    const int parent_level = node_level - count;
+    if (parent_level < 0) {
+      record_error(sc, kStageOctree, 1);
+      continue;
+    }
+    uint32_t key;
+    if (r < g) {
+      key = ws.uniq[r];
+    } else {
+      const int f = ws.rfirst[r - g];
+      if (f < 0 || f >= g) {
+        record_error(sc, kStageOctree, 7);
+        continue;
+      }
+      key = ws.uniq[f];
+    }
+    int parent_node = 0;
+    int anc = ws.rparent[r];
+    int iters = 0;
+    bool bad = false;
+    while (anc != -1) {
+      if (anc < 0 || anc >= nr) {
+        record_error(sc, kStageOctree, 2);
+        bad = true;
+        break;
+      }
+      const int ac = ws.pcount[anc];
+      if (ac > 0) {
+        if (ws.plevel[anc] != parent_level) {
+          record_error(sc, kStageOctree, 3);
+          bad = true;
+          break;
+        }
+        parent_node = 1 + ws.poffset[anc] + ac - 1;
+        break;
+      }
+      anc = ws.rparent[anc];
+      if (++iters > nr) {
+        record_error(sc, kStageOctree, 2);
+        bad = true;
+        break;
+      }
+    }
+    if (bad) continue;
+    if (anc == -1 && parent_level != 0) {
+      record_error(sc, kStageOctree, 3);
+      continue;
+    }
+    if (parent_node < 0 || parent_node >= m) {
+      record_error(sc, kStageOctree, 6);
+      continue;
+    }
+    const int first_node = 1 + ws.poffset[r];
+    for (int local = 0; local < count; ++local) {
+      const int node = first_node + local;
+      if (node <= 0 || node >= m) {
+        record_error(sc, kStageOctree, 6);
+        bad = true;
+        break;
+      }
+      const int level = parent_level + local + 1;
+      const int par = (local == 0) ? parent_node : node - 1;
+      ws.olevel[node] = level;
+      ws.oprefix[node] = prefix_at_level(key, level);
+      ws.oparent[node] = par;
+      const int prev = atomicCAS(&ws.children[(size_t)par * 8 + octant_at_level(key, level)], -1, node);
+      if (prev != -1 && prev != node) {
+        record_error(sc, kStageOctree, 4);
+        bad = true;
+        break;
+      }
+    }
+    if (bad) continue;
+    if (r < g) {
+      const int leaf = first_node + count - 1;
+      const int ll = parent_level + count;
+      if (ll <= 0 || ll > kMaxLevel) {
+        record_error(sc, kStageOctree, 5);
+        continue;
+      }
+      ws.ofirst[leaf] = ws.gfirst[r];
+      ws.ocount[leaf] = ws.gcount[r];
+    }
+  }
+}
+
+// -------------------------------------------- geometry + leaf physics ----
+
+// Per node: cell centre / half size from the Morton prefix path
+// (octree_geometry.cu:56-102), child count (octree_physics.cu:236-265) and,
+// for occupied leaves, mass and centre of mass summed over the group's
+// particles in sorted order (octree_physics.cu:267-326).
+__global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  const double bx = sc->box[0], by = sc->box[1], bz = sc->box[2], bs = sc->box[3];
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    const int level = ws.olevel[node];
+    if (level < 0 || level > kMaxLevel) {
+      record_error(sc, kStageGeometry, 1);
+    } else {
+      const uint32_t prefix = ws.oprefix[node];
+      bool valid = (prefix & ~kSpatialMask) == 0u;
+      if (valid) {
+        if (level == 0) {
+          valid = prefix == 0u;
+        } else {
+          const int rem = kSpatialBits - level * kDims;
+          valid = (prefix & ~(kSpatialMask & (~0u << rem))) == 0u;
+        }
+      }
+      if (!valid) {
+        record_error(sc, kStageGeometry, 2);
+      } else {
+        double cx = bx, cy = by, cz = bz, h = __dmul_rn(bs, 0.5);
+        for (int d = 1; d <= level; ++d) {
+          const int oct = (int)((prefix >> (kSpatialBits - d * kDims)) & 7u);
+          const double ch = __dmul_rn(h, 0.5);
+          cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
+          cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
+          cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
+          h = ch;
+        }
+        ws.cx[node] = cx;
+        ws.cy[node] = cy;
+        ws.cz[node] = cz;
+        ws.half[node] = h;
+      }
+    }
+    const int4 *c4 = reinterpret_cast<const int4 *>(ws.children + (size_t)node * 8);
+    const int4 a = c4[0], b = c4[1];
+    const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    int cnt = 0;
+    bool bad = false;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      if (ch[o] == -1) continue;
+      if (ch[o] <= 0 || ch[o] >= m) bad = true;
+      ++cnt;
+    }
+    if (bad) {
+      record_error(sc, kStagePhysics, 1);
+      continue;
+    }
+    ws.child_count[node] = cnt;
+    const int pc = ws.ocount[node];
+    if (pc > 0 && cnt != 0) record_error(sc, kStagePhysics, 4);
+    if (node == 0) ws.preoff[0] = 0;
+    if (pc <= 0) continue;
+    const int f = ws.ofirst[node];
+    if (f < 0 || f + pc > ws.n) {
+      record_error(sc, kStagePhysics, 2);
+      continue;
+    }
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    for (int k = 0; k < pc; ++k) {
+      const double4 p = ws.pm4[f + k];
+      tm = __dadd_rn(tm, p.w);
+      wx = __fma_rn(p.w, p.x, wx);
+      wy = __fma_rn(p.w, p.y, wy);
+      wz = __fma_rn(p.w, p.z, wz);
+    }
+    ws.mass[node] = tm;
+    if (tm > 0.0) {
+      const double inv = __ddiv_rn(1.0, tm);
+      ws.comx[node] = __dmul_rn(wx, inv);
+      ws.comy[node] = __dmul_rn(wy, inv);
+      ws.comz[node] = __dmul_rn(wz, inv);
+    }
+    ws.subtree[node] = 1;
+  }
+}
+
+// octree_physics.cu:328-417: bottom-up propagation with per-node arrival
+// counters; the last child to arrive combines the children in octant order
+// 0..7 (deterministic).  The same thread also sums subtree sizes and assigns
+// each child its offset within the parent's depth-first preorder (children
+// visited octant 7 -> 0).  Spin-free: a thread that is not last just stops.
+__global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < m; leaf += gridDim.x * blockDim.x) {
+    if (ws.ocount[leaf] <= 0) continue;
+    if (ws.child_count[leaf] != 0) {
+      record_error(sc, kStagePhysics, 4);
+      continue;
+    }
+    int done = leaf;
+    int parent = ws.oparent[done];
+    int climbs = 0;
+    while (parent != -1) {
+      if (parent < 0 || parent >= m || ++climbs > kMaxLevel + 1) {
+        record_error(sc, kStagePhysics, 5);
+        break;
+      }
+      const int required = ws.child_count[parent];
+      if (required <= 0 || required > 8) {
+        record_error(sc, kStagePhysics, 6);
+        break;
+      }
+      __threadfence();
+      const int arrived = atomicAdd(&ws.pending[parent], 1) + 1;
+      if (arrived < required) break;
+      if (arrived > required) {
+        record_error(sc, kStagePhysics, 7);
+        break;
+      }
+      __threadfence();
+      const int4 *c4 = reinterpret_cast<const int4 *>(ws.children + (size_t)parent * 8);
+      const int4 a = c4[0], b = c4[1];
+      const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+      int size = 1;
+      int sub[8];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) {
+        sub[o] = 0;
+        const int c = ch[o];
+        if (c <= 0 || c >= m) continue;
+        const double cm = __ldcg(ws.mass + c);
+        tm = __dadd_rn(tm, cm);
+        wx = __fma_rn(cm, __ldcg(ws.comx + c), wx);
+        wy = __fma_rn(cm, __ldcg(ws.comy + c), wy);
+        wz = __fma_rn(cm, __ldcg(ws.comz + c), wz);
+        sub[o] = __ldcg(ws.subtree + c);
+        size += sub[o];
+      }
+      ws.mass[parent] = tm;
+      if (tm > 0.0) {
+        const double inv = __ddiv_rn(1.0, tm);
+        ws.comx[parent] = __dmul_rn(wx, inv);
+        ws.comy[parent] = __dmul_rn(wy, inv);
+        ws.comz[parent] = __dmul_rn(wz, inv);
+      } else {
+        ws.comx[parent] = 0.0;
+        ws.comy[parent] = 0.0;
+        ws.comz[parent] = 0.0;
+      }
+      int run = 1;
+#pragma unroll
+      for (int o = 7; o >= 0; --o) {
+        if (ch[o] <= 0 || ch[o] >= m) continue;
+        ws.preoff[ch[o]] = run;
+        run += sub[o];
+      }
+      ws.subtree[parent] = size;
+      done = parent;
+      parent = ws.oparent[done];
+    }
+  }
+}
+
+// --------------------------------------------------------------- layout --
+
+// Traversal records in depth-first preorder with children visited octant
+// 7 -> 0 (the reference's traversal order, barnes_hut.cu:110-182): node n sits
+// at pre(n) = sum of the preorder offsets on its path to the root, its
+// subtree ends at pre(n) + size(n) ("skip"), and its children are listed in
+// visit order.  The acceptance radius crit = side/theta + |com - centre|
+// (barnes_hut.cu:297-311) is precomputed once per node, with a +-2^-44 band
+// around crit^2 inside which the traversal falls back to the exact
+// sqrt(d^2) > crit comparison.
+__global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double theta) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    int pre = 0;
+    int v = node;
+    int guard = 0;
+    while (v != 0) {
+      pre += ws.preoff[v];
+      v = ws.oparent[v];
+      if (v < 0 || ++guard > kMaxLevel + 1) {
+        record_error(sc, kStageLayout, 1);
+        break;
+      }
+    }
+    if (v != 0) continue;
+    if (pre < 0 || pre >= m) {
+      record_error(sc, kStageLayout, 1);
+      continue;
+    }
+    const double h = ws.half[node];
+    if (!(h > 0.0)) record_error(sc, kStageTraversal, 8);
+    int pc = ws.ocount[node];
+    const int cnt = ws.child_count[node];
+    const int f = ws.ofirst[node];
+    if (pc > 0 && (f < 0 || f + pc > ws.n)) {
+      record_error(sc, kStageTraversal, 2);
+      pc = 0;
+    }
+    int size = (pc > 0) ? 1 : ws.subtree[node];
+    if (size < 1 || pre + size > m) {
+      record_error(sc, kStageLayout, 1);
+      size = 1;
+    }
+    if (pc > 0 && cnt != 0) record_error(sc, kStageTraversal, 7);
+    const double mass = ws.mass[node];
+    if (pc <= 0 && cnt == 0 && mass != 0.0) record_error(sc, kStageTraversal, 5);
+    const double comx = ws.comx[node], comy = ws.comy[node], comz = ws.comz[node];
+    const double cx = ws.cx[node], cy = ws.cy[node], cz = ws.cz[node];
+    ws.node_a[pre] = make_double4(comx, comy, comz, mass);
+    ws.node_b[pre] = make_double4(cx, cy, cz, h);
+    const double side = __dmul_rn(2.0, h);
+    const double ox = __dsub_rn(comx, cx), oy = __dsub_rn(comy, cy), oz = __dsub_rn(comz, cz);
+    const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
+    const double crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
+    const double c2 = __dmul_rn(crit, crit);
+    ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), 0.0);
+    int j = 0;
+    int *kids = ws.node_kids + (size_t)pre * 8;
+    for (int o = 7; o >= 0; --o) {
+      const int c = ws.children[(size_t)node * 8 + o];
+      if (c <= 0 || c >= m) continue;
+      kids[j++] = pre + ws.preoff[c];
+    }
+    ws.node_meta[pre] = make_int4(pre + size, pc > 0 ? f : -1, pc > 0 ? pc : 0, j);
+    for (; j < 8; ++j) kids[j] = -1;
+  }
+}
+
+// Reference-layout keys only (no particles): used by the function-level
+// topology entry points.
+__global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x)
+    ws.pairs_a[i] = ((unsigned long long)keys[i] << 32) | (unsigned)i;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ launches ---
+
+cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  count_launches(1);
+  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kSortPasses * 256, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)kSortPasses * ws.sort_tiles * 256, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.scan_status, 0,
+                      sizeof(unsigned long long) * (size_t)(ws.scan_tiles_n + ws.scan_tiles_r), s);
+  if (e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kd_bbox(Workspace &ws, double dt, int do_kd, cudaStream_t s) {
+  int blocks = (ws.n + kBlock - 1) / kBlock;
+  const int cap = grid_for(ws, 4);
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  kd_bbox_kernel<<<blocks, kBlock, 0, s>>>(ws, dt, do_kd);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s) {
+  int blocks = (ws.n + kBlock - 1) / kBlock;
+  const int cap = grid_for(ws, 4);
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
+  unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
+  for (int p = 0; p < kSortPasses; ++p) {
+    onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
+        src, dst, ws.n, p, ws.digit_hist, ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
+    unsigned long long *t = src;
+    src = dst;
+    dst = t;
+  }
+  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, 1);
+  count_launches(2 + kSortPasses);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
+  const int grid = grid_for(ws, 8);
+  karras_kernel<<<grid, kBlock, 0, s>>>(ws);
+  plan_kernel<<<ws.scan_tiles_r, kScanThreads, 0, s>>>(ws);
+  octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
+  materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
+  node_init_kernel<<<grid, kBlock, 0, s>>>(ws);
+  propagate_kernel<<<grid, kBlock, 0, s>>>(ws);
+  layout_kernel<<<grid, kBlock, 0, s>>>(ws, theta);
+  count_launches(7);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys, cudaStream_t s) {
+  pack_keys_kernel<<<grid_for(ws, 4), kBlock, 0, s>>>(ws, sorted_keys);
+  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, 0);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_topology(Workspace &ws, cudaStream_t s) {
+  const int grid = grid_for(ws, 8);
+  karras_kernel<<<grid, kBlock, 0, s>>>(ws);
+  plan_kernel<<<ws.scan_tiles_r, kScanThreads, 0, s>>>(ws);
+  octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
+  materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
+  count_launches(4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_radix_tree_only(const uint32_t *keys, int n, int *left, int *right, int *rfirst,
+                                   int *rlast, int *plen, int *parent, cudaStream_t s) {
+  int blocks = (n + kBlock - 1) / kBlock;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 4096) blocks = 4096;
+  karras_only_kernel<<<blocks, kBlock, 0, s>>>(keys, n, left, right, rfirst, rlast, plen, parent);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace nbb

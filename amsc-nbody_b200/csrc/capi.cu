@@ -1,0 +1,865 @@
+// capi.cu -- the C ABI of include/nbb.h over the build and traversal kernels.
+//
+// Ownership and error behaviour follow the reference's Simulation
+// (src/simulation.cpp, paths relative to the sytrams/AMSC-Nbody project
+// root): the handle owns every device buffer, all of them allocated once at
+// creation; a step allocates nothing, never synchronises with the host
+// inside, and is captured once into a CUDA graph that later steps replay.
+#include "nbb.h"
+#include "nbb_internal.cuh"
+
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace nbb {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+uint64_t launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+cudaError_t configure_traversal(Workspace &ws);
+
+}  // namespace nbb
+
+using namespace nbb;
+
+namespace {
+
+thread_local std::string t_message;
+thread_local int t_code = 0;
+
+int fail(int status, const std::string &msg, int code = 0) {
+  t_message = msg;
+  t_code = code;
+  return status;
+}
+
+int ok() {
+  t_message.clear();
+  t_code = 0;
+  return NBB_OK;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+    return fail(NBB_ERR_NO_DEVICE, std::string(what) + ": " + cudaGetErrorString(e), (int)e);
+  return fail(NBB_ERR_CUDA, std::string(what) + " failed: " + cudaGetErrorString(e), (int)e);
+}
+
+#define NBB_CUDA(call, what)                 \
+  do {                                       \
+    cudaError_t _e = (call);                 \
+    if (_e != cudaSuccess) return cuda_fail(_e, what); \
+  } while (0)
+
+// Messages of the reference's device error codes, by stage.
+const char *device_message(int stage, int code) {
+  if (code == kCodeTimeout) return "A bounded device-side wait gave up (look-back predecessor never published)";
+  switch (stage) {
+    case kStageBbox:
+      return code == 1 ? "Particle positions must be finite to compute a bounding box."
+                       : "Morton bounding box is not valid";
+    case kStagePlan:  // radix_to_octree.cu:102-121
+      switch (code) {
+        case 1: return "A Morton key uses bits outside the configured 30-bit spatial layout";
+        case 2: return "A radix node has an invalid parent";
+        case 3: return "A radix child has an octree level smaller than its parent";
+        case 4: return "A radix internal node has an invalid prefix length";
+        case kCodeOverflow: return "The computed octree node count exceeds the node capacity";
+        default: return "Unknown radix-to-octree planning error";
+      }
+    case kStageOctree:  // octree_builder.cu:206-234
+      switch (code) {
+        case 1: return "Invalid radix edge metadata";
+        case 2: return "Invalid radix ancestor while constructing octree";
+        case 3: return "Could not find the correct octree parent level";
+        case 4: return "Two octree nodes attempted to occupy the same parent octant";
+        case 5: return "A radix leaf terminates at an invalid octree level";
+        case 6: return "Generated octree node ID is outside the allocated range";
+        case 7: return "Invalid representative Morton key";
+        default: return "Unknown sparse-octree construction error";
+      }
+    case kStageGeometry:  // octree_geometry.cu:21-34
+      return code == 1 ? "Octree node has an invalid level"
+                       : code == 2 ? "Octree node has an invalid Morton prefix" : "Unknown octree geometry error";
+    case kStagePhysics:  // octree_physics.cu:190-218
+      switch (code) {
+        case 1: return "Octree contains an invalid child ID";
+        case 2: return "Occupied octree leaf has invalid particle range";
+        case 3: return "Sorted particle index is outside the particle array";
+        case 4: return "Occupied octree leaf has children";
+        case 5: return "Invalid octree parent during bottom-up propagation";
+        case 6: return "Invalid octree child count";
+        case 7: return "An octree parent was signalled too many times";
+        default: return "Unknown octree physics error";
+      }
+    case kStageTraversal:  // barnes_hut.cu:41-72
+      switch (code) {
+        case 1: return "Barnes-Hut traversal found an invalid child node";
+        case 2: return "Barnes-Hut traversal found an invalid leaf particle range";
+        case 3: return "Sorted particle index is outside the particle array";
+        case 4: return "Barnes-Hut traversal found inconsistent parent-child topology";
+        case 5: return "Barnes-Hut traversal found an empty terminal node";
+        case 6: return "Singular gravitational interaction; use positive softening";
+        case 7: return "Occupied octree leaf unexpectedly has children";
+        case 8: return "Octree node has invalid geometry";
+        default: return "Unknown Barnes-Hut traversal error";
+      }
+    case kStageLayout:
+      return "Octree preorder layout found an inconsistent parent chain";
+    default:
+      return "Unknown device error";
+  }
+}
+
+int device_status(int word) {
+  const int stage = word / 100, code = word % 100;
+  const int status = (code == kCodeTimeout) ? NBB_ERR_TIMEOUT
+                     : (stage == kStageBbox && code == 1) ? NBB_ERR_DOMAIN
+                     : (stage == kStagePlan && code == kCodeOverflow) ? NBB_ERR_OVERFLOW
+                                                                      : NBB_ERR_DEVICE;
+  return fail(status, device_message(stage, code), word);
+}
+
+// Octree node capacity: every level L holds at most min(8^L, G) nodes and
+// G <= n, over levels 0..10.
+int node_capacity(int n) {
+  long long cap = 1;
+  long long width = 1;
+  for (int level = 0; level <= kMaxLevel; ++level) {
+    cap += (width < n) ? width : n;
+    if (width < (1ll << 40)) width *= 8;
+  }
+  return cap > INT_MAX ? INT_MAX : (int)cap;
+}
+
+struct Allocation {
+  std::vector<void *> ptrs;
+  ~Allocation() {
+    for (void *p : ptrs) cudaFree(p);
+  }
+  template <typename T>
+  cudaError_t get(T *&out, size_t count) {
+    void *p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, (count > 0 ? count : 1) * sizeof(T));
+    if (e != cudaSuccess) return e;
+    ptrs.push_back(p);
+    out = static_cast<T *>(p);
+    return cudaSuccess;
+  }
+};
+
+// Allocate every buffer of a workspace for n particles (state included when
+// with_state).  All device memory is taken here; nothing is allocated later.
+cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_state) {
+  ws = Workspace{};
+  ws.n = n;
+  ws.cap_nodes = node_capacity(n);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&ws.num_sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t N = (size_t)n, C = (size_t)ws.cap_nodes;
+  cudaError_t e = cudaSuccess;
+#define GET(ptr, cnt) \
+  if ((e = al.get(ptr, cnt)) != cudaSuccess) return e
+  if (with_state) {
+    GET(ws.m, N); GET(ws.x, N); GET(ws.y, N); GET(ws.z, N);
+    GET(ws.vx, N); GET(ws.vy, N); GET(ws.vz, N);
+    GET(ws.ax, N); GET(ws.ay, N); GET(ws.az, N);
+    GET(ws.type, N);
+  }
+  GET(ws.sc, 1);
+  GET(ws.pairs_a, N); GET(ws.pairs_b, N);
+  GET(ws.digit_hist, (size_t)kSortPasses * 256);
+  ws.sort_tiles = (n + kSortTile - 1) / kSortTile;
+  GET(ws.sort_status, (size_t)kSortPasses * ws.sort_tiles * 256);
+  ws.scan_tiles_n = (n + kScanTile - 1) / kScanTile;
+  ws.scan_tiles_r = (2 * n - 1 + kScanTile - 1) / kScanTile;
+  GET(ws.scan_status, (size_t)(ws.scan_tiles_n + ws.scan_tiles_r));
+  GET(ws.keys, N); GET(ws.idx, N); GET(ws.pm4, N);
+  GET(ws.uniq, N); GET(ws.gfirst, N); GET(ws.gcount, N); GET(ws.glast, N);
+  GET(ws.left, N); GET(ws.right, N); GET(ws.rfirst, N); GET(ws.rlast, N); GET(ws.plen, N);
+  GET(ws.rparent, 2 * N);
+  GET(ws.plevel, 2 * N); GET(ws.pcount, 2 * N); GET(ws.poffset, 2 * N);
+  GET(ws.children, 8 * C);
+  GET(ws.oparent, C); GET(ws.olevel, C); GET(ws.oprefix, C); GET(ws.ofirst, C); GET(ws.ocount, C);
+  GET(ws.child_count, C); GET(ws.pending, C); GET(ws.subtree, C); GET(ws.preoff, C);
+  GET(ws.cx, C); GET(ws.cy, C); GET(ws.cz, C); GET(ws.half, C);
+  GET(ws.mass, C); GET(ws.comx, C); GET(ws.comy, C); GET(ws.comz, C);
+  GET(ws.node_a, C); GET(ws.node_b, C); GET(ws.node_c, C); GET(ws.node_meta, C);
+  GET(ws.node_kids, 8 * C);
+#undef GET
+  e = cudaMemset(ws.sc, 0, sizeof(DevScalars));
+  if (e != cudaSuccess) return e;
+  return configure_traversal(ws);
+}
+
+bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
+
+template <typename T>
+cudaError_t d2h_opt(T *dst, const T *src, size_t count, cudaStream_t s) {
+  if (dst == nullptr || count == 0) return cudaSuccess;
+  return cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, s);
+}
+
+// Copy every intermediate of the last build into caller buffers.
+int export_workspace(const Workspace &ws, nbb_tree_export *o, cudaStream_t s, bool particles) {
+  DevScalars sc;
+  NBB_CUDA(cudaMemcpyAsync(&sc, ws.sc, sizeof(sc), cudaMemcpyDeviceToHost, s), "copy device scalars");
+  NBB_CUDA(cudaStreamSynchronize(s), "export synchronisation");
+  const int n = ws.n, g = sc.n_groups, m = sc.n_nodes;
+  o->n_groups = g;
+  o->n_octree = m;
+  for (int a = 0; a < 4; ++a) o->box[a] = sc.box[a];
+  if (m > o->m_capacity && (o->children || o->oparent || o->olevel || o->oprefix || o->ofirst ||
+                            o->ocount || o->child_count || o->cx || o->mass))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "export m_capacity is smaller than the octree node count");
+  const size_t G = (size_t)g, R = g > 0 ? (size_t)(2 * g - 1) : 0, I = g > 1 ? (size_t)(g - 1) : 0;
+  const size_t M = (size_t)m;
+  NBB_CUDA(d2h_opt(o->keys, ws.keys, (size_t)n, s), "export keys");
+  NBB_CUDA(d2h_opt(o->idx, ws.idx, (size_t)n, s), "export idx");
+  NBB_CUDA(d2h_opt(o->uniq, ws.uniq, G, s), "export groups");
+  NBB_CUDA(d2h_opt(o->gfirst, ws.gfirst, G, s), "export groups");
+  NBB_CUDA(d2h_opt(o->gcount, ws.gcount, G, s), "export groups");
+  NBB_CUDA(d2h_opt(o->left, ws.left, I, s), "export tree");
+  NBB_CUDA(d2h_opt(o->right, ws.right, I, s), "export tree");
+  NBB_CUDA(d2h_opt(o->rfirst, ws.rfirst, I, s), "export tree");
+  NBB_CUDA(d2h_opt(o->rlast, ws.rlast, I, s), "export tree");
+  NBB_CUDA(d2h_opt(o->plen, ws.plen, I, s), "export tree");
+  NBB_CUDA(d2h_opt(o->rparent, ws.rparent, R, s), "export tree");
+  NBB_CUDA(d2h_opt(o->plan_level, ws.plevel, R, s), "export plan");
+  NBB_CUDA(d2h_opt(o->plan_count, ws.pcount, R, s), "export plan");
+  NBB_CUDA(d2h_opt(o->plan_offset, ws.poffset, R, s), "export plan");
+  NBB_CUDA(d2h_opt(o->children, ws.children, 8 * M, s), "export octree");
+  NBB_CUDA(d2h_opt(o->oparent, ws.oparent, M, s), "export octree");
+  NBB_CUDA(d2h_opt(o->olevel, ws.olevel, M, s), "export octree");
+  NBB_CUDA(d2h_opt(o->oprefix, ws.oprefix, M, s), "export octree");
+  NBB_CUDA(d2h_opt(o->ofirst, ws.ofirst, M, s), "export octree");
+  NBB_CUDA(d2h_opt(o->ocount, ws.ocount, M, s), "export octree");
+  if (particles) {
+    NBB_CUDA(d2h_opt(o->child_count, ws.child_count, M, s), "export octree");
+    NBB_CUDA(d2h_opt(o->cx, ws.cx, M, s), "export geometry");
+    NBB_CUDA(d2h_opt(o->cy, ws.cy, M, s), "export geometry");
+    NBB_CUDA(d2h_opt(o->cz, ws.cz, M, s), "export geometry");
+    NBB_CUDA(d2h_opt(o->half, ws.half, M, s), "export geometry");
+    NBB_CUDA(d2h_opt(o->mass, ws.mass, M, s), "export physics");
+    NBB_CUDA(d2h_opt(o->comx, ws.comx, M, s), "export physics");
+    NBB_CUDA(d2h_opt(o->comy, ws.comy, M, s), "export physics");
+    NBB_CUDA(d2h_opt(o->comz, ws.comz, M, s), "export physics");
+  }
+  NBB_CUDA(cudaStreamSynchronize(s), "export synchronisation");
+  return ok();
+}
+
+// Read the sticky device error word (one small copy + stream sync).
+int check_device(const Workspace &ws, cudaStream_t s) {
+  int word = 0;
+  NBB_CUDA(cudaMemcpyAsync(&word, &ws.sc->error, sizeof(int), cudaMemcpyDeviceToHost, s), "copy error word");
+  NBB_CUDA(cudaStreamSynchronize(s), "device synchronisation");
+  if (word != 0) return device_status(word);
+  return ok();
+}
+
+// Rebuild + force on the workspace state (kd: first half kick + drift before
+// the rebuild; kick: second half kick fused into the traversal).
+cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, double dt, int kd,
+                                  cudaStream_t s) {
+  cudaError_t e = launch_step_reset(ws, s);
+  if (e == cudaSuccess) e = launch_kd_bbox(ws, dt, kd, s);
+  if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
+  if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
+  if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
+  return e;
+}
+
+template <typename T>
+cudaError_t stage_in(const T *src, size_t count, bool on_device, Allocation &al, const T *&dst,
+                            cudaStream_t s) {
+  if (src == nullptr || on_device) {
+    dst = src;
+    return cudaSuccess;
+  }
+  T *d = nullptr;
+  cudaError_t e = al.get(d, count);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(d, src, count * sizeof(T), cudaMemcpyHostToDevice, s);
+  dst = d;
+  return e;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------- handle ---
+
+struct nbb_sim {
+  nbb_config cfg{};
+  Workspace ws{};
+  Allocation alloc;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  enum class State { created, ready, failed } state = State::created;
+  double time = 0.0;
+  uint64_t steps = 0;
+  cudaGraphExec_t step_graph = nullptr;
+  cudaGraph_t step_graph_def = nullptr;
+  uint64_t graph_kernels = 0;
+};
+
+extern "C" {
+
+void nbb_config_default(nbb_config *cfg) {
+  if (!cfg) return;
+  cfg->time_step = 0.0;
+  cfg->theta = 0.5;                        // barnes_hut.hpp:10
+  cfg->softening = 1.0e-6;                 // barnes_hut.hpp:11
+  cfg->gravitational_constant = 6.67430e-11;  // barnes_hut.hpp:12
+  cfg->precision = NBB_PRECISION_FP64;
+  cfg->group_size = 0;
+  cfg->use_graph = 1;
+  cfg->device = 0;
+}
+
+int nbb_measure_fma_tflops(int precision, double *tflops) {
+  if (!tflops) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  NBB_CUDA(measure_fma_tflops(precision, tflops), "FMA throughput kernel");
+  return ok();
+}
+
+const char *nbb_last_error_message(void) { return t_message.c_str(); }
+int nbb_last_error_code(void) { return t_code; }
+uint64_t nbb_kernel_launch_count(void) { return nbb::launch_count(); }
+
+static int validate_config(const nbb_config *c) {
+  // simulation.cpp:21-33, barnes_hut.cu:376-383
+  if (!std::isfinite(c->time_step) || c->time_step <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation timeStep must be finite and positive");
+  if (!finite_nonneg(c->theta))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation theta must be finite and non-negative");
+  if (!finite_nonneg(c->softening))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation softening must be finite and non-negative");
+  if (!std::isfinite(c->gravitational_constant) || c->gravitational_constant <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Gravitational constant must be finite and positive");
+  if (c->precision != NBB_PRECISION_FP64 && c->precision != NBB_PRECISION_MIXED)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown traversal precision");
+  return NBB_OK;
+}
+
+int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const double *x,
+                   const double *y, const double *z, const double *vx, const double *vy,
+                   const double *vz, const uint8_t *type, int on_device, nbb_sim **out) {
+  if (!cfg || !out) return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_sim_create: null argument");
+  *out = nullptr;
+  int st = validate_config(cfg);
+  if (st) return st;
+  if (n == 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation requires at least one particle");
+  if (n > (size_t)(INT_MAX / 2))
+    return fail(NBB_ERR_OVERFLOW, "Particle count exceeds the tree representation");
+  if (!mass || !x || !y || !z || !vx || !vy || !vz)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Particle arrays must not be null");
+  NBB_CUDA(cudaSetDevice(cfg->device), "cudaSetDevice");
+  nbb_sim *sim = new (std::nothrow) nbb_sim();
+  if (!sim) return fail(NBB_ERR_CUDA, "host allocation failed");
+  sim->cfg = *cfg;
+  cudaError_t e = cudaStreamCreateWithFlags(&sim->own_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = alloc_workspace(sim->ws, sim->alloc, (int)n, true);
+  if (e != cudaSuccess) {
+    if (sim->own_stream) cudaStreamDestroy(sim->own_stream);
+    delete sim;
+    return cuda_fail(e, "allocate simulation state");
+  }
+  sim->stream = sim->own_stream;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const size_t bytes = n * sizeof(double);
+  Workspace &ws = sim->ws;
+  const double *src[7] = {mass, x, y, z, vx, vy, vz};
+  double *dst[7] = {ws.m, ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz};
+  for (int k = 0; k < 7 && e == cudaSuccess; ++k) e = cudaMemcpyAsync(dst[k], src[k], bytes, kind, sim->stream);
+  if (e == cudaSuccess) e = type ? cudaMemcpyAsync(ws.type, type, n, kind, sim->stream)
+                                 : cudaMemsetAsync(ws.type, 0, n, sim->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.ax, 0, bytes, sim->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.ay, 0, bytes, sim->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ws.az, 0, bytes, sim->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
+  if (e != cudaSuccess) {
+    nbb_sim_destroy(sim);
+    return cuda_fail(e, "copy particle state");
+  }
+  *out = sim;
+  return ok();
+}
+
+static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
+  TraversalParams tp;
+  tp.theta = sim->cfg.theta;
+  tp.soft = sim->cfg.softening;
+  tp.g = sim->cfg.gravitational_constant;
+  tp.half_dt = 0.5 * sim->cfg.time_step;
+  tp.kick = kick;
+  tp.precision = sim->cfg.precision;
+  tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size : 32;
+  return tp;
+}
+
+int nbb_sim_initialize(nbb_sim *sim) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (sim->state != nbb_sim::State::created)
+    return fail(NBB_ERR_LOGIC, "Simulation can only be initialized once");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  Workspace &ws = sim->ws;
+  cudaError_t e = enqueue_rebuild_force(ws, traversal_params(sim, 0), sim->cfg.time_step, 0, sim->stream);
+  if (e != cudaSuccess) {
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "initialize");
+  }
+  const int st = check_device(ws, sim->stream);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  sim->state = nbb_sim::State::ready;
+  return ok();
+}
+
+// Capture one step (reset, KD + bbox, Morton + sort + groups, tree,
+// traversal + K) into a graph on the handle's own stream.
+static cudaError_t capture_step(nbb_sim *sim) {
+  Workspace &ws = sim->ws;
+  const uint64_t before = nbb::launch_count();
+  cudaError_t e = cudaStreamBeginCapture(sim->own_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t body = enqueue_rebuild_force(ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->own_stream);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(sim->own_stream, &graph);
+  sim->graph_kernels = nbb::launch_count() - before;
+  // kernels recorded during capture did not run; count them per replay
+  nbb::count_launches((uint64_t)0 - sim->graph_kernels);
+  if (body != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return body;
+  }
+  if (e != cudaSuccess) return e;
+  e = cudaGraphInstantiate(&sim->step_graph, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return e;
+  }
+  sim->step_graph_def = graph;
+  return cudaSuccess;
+}
+
+static int run_steps(nbb_sim *sim, uint64_t steps, const char *what) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (sim->state != nbb_sim::State::ready) return fail(NBB_ERR_LOGIC, what);
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  Workspace &ws = sim->ws;
+  cudaError_t e = cudaSuccess;
+  if (steps > 0 && sim->cfg.use_graph && !sim->step_graph) e = capture_step(sim);
+  for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+    if (sim->step_graph) {
+      e = cudaGraphLaunch(sim->step_graph, sim->stream);
+      nbb::count_launches(sim->graph_kernels);
+    } else {
+      e = enqueue_rebuild_force(ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->stream);
+    }
+  }
+  if (e != cudaSuccess) {
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "step");
+  }
+  const int st = check_device(ws, sim->stream);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  sim->time += sim->cfg.time_step * (double)steps;
+  sim->steps += steps;
+  return ok();
+}
+
+int nbb_sim_step(nbb_sim *sim) { return run_steps(sim, 1, "Simulation must be initialized before stepping"); }
+
+int nbb_sim_run(nbb_sim *sim, uint64_t steps) {
+  return run_steps(sim, steps, "Simulation must be initialized before running");
+}
+
+double nbb_sim_time(const nbb_sim *sim) { return sim ? sim->time : 0.0; }
+uint64_t nbb_sim_step_number(const nbb_sim *sim) { return sim ? sim->steps : 0; }
+
+int nbb_sim_state(nbb_sim *sim, nbb_state_view *v) {
+  if (!sim || !v) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  const Workspace &ws = sim->ws;
+  v->count = (size_t)ws.n;
+  v->mass = ws.m; v->x = ws.x; v->y = ws.y; v->z = ws.z;
+  v->vx = ws.vx; v->vy = ws.vy; v->vz = ws.vz;
+  v->type = ws.type;
+  v->ax = ws.ax; v->ay = ws.ay; v->az = ws.az;
+  return ok();
+}
+
+int nbb_sim_upload(nbb_sim *sim, const double *mass, const double *x, const double *y, const double *z,
+                   const double *vx, const double *vy, const double *vz) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  Workspace &ws = sim->ws;
+  const size_t bytes = (size_t)ws.n * sizeof(double);
+  const double *src[7] = {mass, x, y, z, vx, vy, vz};
+  double *dst[7] = {ws.m, ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz};
+  for (int k = 0; k < 7; ++k)
+    if (src[k]) NBB_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyHostToDevice, sim->stream), "upload");
+  return ok();
+}
+
+int nbb_sim_download(nbb_sim *sim, double *x, double *y, double *z, double *vx, double *vy, double *vz) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  Workspace &ws = sim->ws;
+  const size_t bytes = (size_t)ws.n * sizeof(double);
+  double *dst[6] = {x, y, z, vx, vy, vz};
+  const double *src[6] = {ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz};
+  for (int k = 0; k < 6; ++k)
+    if (dst[k]) NBB_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyDeviceToHost, sim->stream), "download");
+  NBB_CUDA(cudaStreamSynchronize(sim->stream), "download synchronisation");
+  return ok();
+}
+
+int nbb_sim_download_accel(nbb_sim *sim, double *ax, double *ay, double *az) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  Workspace &ws = sim->ws;
+  const size_t bytes = (size_t)ws.n * sizeof(double);
+  double *dst[3] = {ax, ay, az};
+  const double *src[3] = {ws.ax, ws.ay, ws.az};
+  for (int k = 0; k < 3; ++k)
+    if (dst[k]) NBB_CUDA(cudaMemcpyAsync(dst[k], src[k], bytes, cudaMemcpyDeviceToHost, sim->stream), "download");
+  NBB_CUDA(cudaStreamSynchronize(sim->stream), "download synchronisation");
+  return ok();
+}
+
+int nbb_sim_set_stream(nbb_sim *sim, void *stream) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  sim->stream = stream ? (cudaStream_t)stream : sim->own_stream;
+  return ok();
+}
+
+int nbb_sim_synchronize(nbb_sim *sim) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  NBB_CUDA(cudaStreamSynchronize(sim->stream), "synchronise");
+  return ok();
+}
+
+int nbb_sim_destroy(nbb_sim *sim) {
+  if (!sim) return ok();
+  cudaSetDevice(sim->cfg.device);
+  if (sim->stream) cudaStreamSynchronize(sim->stream);
+  if (sim->step_graph) cudaGraphExecDestroy(sim->step_graph);
+  if (sim->step_graph_def) cudaGraphDestroy(sim->step_graph_def);
+  cudaStream_t s = sim->own_stream;
+  delete sim;  // frees every device buffer
+  if (s) cudaStreamDestroy(s);
+  return ok();
+}
+
+int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats) {
+  if (!sim || !stats) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  DevScalars sc;
+  NBB_CUDA(cudaMemcpyAsync(&sc, sim->ws.sc, sizeof(sc), cudaMemcpyDeviceToHost, sim->stream), "stats");
+  NBB_CUDA(cudaStreamSynchronize(sim->stream), "stats");
+  stats->n_groups = sc.n_groups;
+  stats->n_octree_nodes = sc.n_nodes;
+  stats->interactions = (int64_t)sc.interactions;
+  stats->mac_tests = (int64_t)sc.mac_tests;
+  return ok();
+}
+
+int nbb_sim_profile(nbb_sim *sim, float *stage_ms, nbb_stats *stats) {
+  if (!sim || !stage_ms) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  if (sim->state != nbb_sim::State::ready)
+    return fail(NBB_ERR_LOGIC, "Simulation must be initialized before profiling");
+  Workspace &ws = sim->ws;
+  cudaStream_t s = sim->stream;
+  cudaEvent_t ev[NBB_PROFILE_STAGES + 1] = {};
+  for (auto &e : ev) NBB_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+  const TraversalParams tp = traversal_params(sim, 0);
+  cudaError_t e = cudaEventRecord(ev[0], s);
+  if (e == cudaSuccess) e = launch_step_reset(ws, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[1], s);
+  if (e == cudaSuccess) e = launch_kd_bbox(ws, sim->cfg.time_step, 0, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
+  if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[3], s);
+  if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[4], s);
+  if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[5], s);
+  if (e == cudaSuccess) e = cudaEventSynchronize(ev[5]);
+  for (int k = 0; k < NBB_PROFILE_STAGES && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&stage_ms[k], ev[k], ev[k + 1]);
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (e != cudaSuccess) {
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "profile");
+  }
+  int st = check_device(ws, s);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  if (stats) return nbb_sim_stats(sim, stats);
+  return ok();
+}
+
+int nbb_sim_export(nbb_sim *sim, nbb_tree_export *out) {
+  if (!sim || !out) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  if (sim->state == nbb_sim::State::created)
+    return fail(NBB_ERR_LOGIC, "Simulation spatial/device state is not available");
+  return export_workspace(sim->ws, out, sim->stream, true);
+}
+
+// ------------------------------------------------------- function level ---
+
+// A temporary workspace on its own stream for the one-shot entry points.
+struct Scratch {
+  Workspace ws{};
+  Allocation al;
+  cudaStream_t s = nullptr;
+  ~Scratch() {
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+int nbb_accel(size_t n, const double *mass, const double *x, const double *y, const double *z, double theta,
+              double softening, double g, int precision, double *ax, double *ay, double *az, int on_device,
+              nbb_tree_export *export_out, nbb_stats *stats) {
+  if (n == 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Cannot compute a bounding box for an empty particle set.");
+  if (n > (size_t)(INT_MAX / 2)) return fail(NBB_ERR_OVERFLOW, "Particle count exceeds the tree representation");
+  if (!mass || !x || !y || !z) return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut particle arrays must not be null");
+  if (!finite_nonneg(theta)) return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut theta must be finite and non-negative");
+  if (!finite_nonneg(softening))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut softening must be finite and non-negative");
+  if (!std::isfinite(g) || g <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Gravitational constant must be finite and positive");
+  if (precision != NBB_PRECISION_FP64 && precision != NBB_PRECISION_MIXED)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown traversal precision");
+  Scratch sc;
+  NBB_CUDA(cudaStreamCreateWithFlags(&sc.s, cudaStreamNonBlocking), "create stream");
+  NBB_CUDA(alloc_workspace(sc.ws, sc.al, (int)n, true), "allocate workspace");
+  Workspace &ws = sc.ws;
+  const cudaMemcpyKind in = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const size_t bytes = n * sizeof(double);
+  NBB_CUDA(cudaMemcpyAsync(ws.m, mass, bytes, in, sc.s), "copy mass");
+  NBB_CUDA(cudaMemcpyAsync(ws.x, x, bytes, in, sc.s), "copy x");
+  NBB_CUDA(cudaMemcpyAsync(ws.y, y, bytes, in, sc.s), "copy y");
+  NBB_CUDA(cudaMemcpyAsync(ws.z, z, bytes, in, sc.s), "copy z");
+  TraversalParams tp;
+  tp.theta = theta;
+  tp.soft = softening;
+  tp.g = g;
+  tp.precision = precision;
+  NBB_CUDA(enqueue_rebuild_force(ws, tp, 0.0, 0, sc.s), "Barnes-Hut evaluation");
+  int st = check_device(ws, sc.s);
+  if (st) return st;
+  if (ax || ay || az) {
+    const cudaMemcpyKind outk = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (ax) NBB_CUDA(cudaMemcpyAsync(ax, ws.ax, bytes, outk, sc.s), "copy ax");
+    if (ay) NBB_CUDA(cudaMemcpyAsync(ay, ws.ay, bytes, outk, sc.s), "copy ay");
+    if (az) NBB_CUDA(cudaMemcpyAsync(az, ws.az, bytes, outk, sc.s), "copy az");
+  }
+  if (stats) {
+    DevScalars d;
+    NBB_CUDA(cudaMemcpyAsync(&d, ws.sc, sizeof(d), cudaMemcpyDeviceToHost, sc.s), "stats");
+    NBB_CUDA(cudaStreamSynchronize(sc.s), "stats");
+    stats->n_groups = d.n_groups;
+    stats->n_octree_nodes = d.n_nodes;
+    stats->interactions = (int64_t)d.interactions;
+    stats->mac_tests = (int64_t)d.mac_tests;
+  }
+  if (export_out) {
+    st = export_workspace(ws, export_out, sc.s, true);
+    if (st) return st;
+  }
+  NBB_CUDA(cudaStreamSynchronize(sc.s), "Barnes-Hut evaluation");
+  return ok();
+}
+
+int nbb_accel_direct(size_t n, const double *mass, const double *x, const double *y, const double *z,
+                     int n_targets, const int *targets, double g, double softening, double *ax, double *ay,
+                     double *az, int on_device) {
+  if (n == 0 || n > (size_t)INT_MAX) return fail(NBB_ERR_INVALID_ARGUMENT, "invalid particle count");
+  if (!mass || !x || !y || !z || !ax || !ay || !az) return fail(NBB_ERR_INVALID_ARGUMENT, "null array");
+  if (!targets) n_targets = (int)n;
+  if (n_targets <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "invalid target count");
+  Allocation al;
+  cudaStream_t s = nullptr;
+  NBB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  const double *dm, *dx, *dy, *dz;
+  const int *dt = nullptr;
+  cudaError_t e = stage_in(mass, n, on_device, al, dm, s);
+  if (e == cudaSuccess) e = stage_in(x, n, on_device, al, dx, s);
+  if (e == cudaSuccess) e = stage_in(y, n, on_device, al, dy, s);
+  if (e == cudaSuccess) e = stage_in(z, n, on_device, al, dz, s);
+  if (e == cudaSuccess && targets) e = stage_in(targets, (size_t)n_targets, on_device, al, dt, s);
+  double *oa[3] = {ax, ay, az};
+  double *da[3] = {ax, ay, az};
+  for (int k = 0; k < 3 && e == cudaSuccess && !on_device; ++k) e = al.get(da[k], (size_t)n_targets);
+  if (e == cudaSuccess) e = launch_direct(n, dm, dx, dy, dz, n_targets, dt, g, softening, da[0], da[1], da[2], s);
+  for (int k = 0; k < 3 && e == cudaSuccess && !on_device; ++k)
+    e = cudaMemcpyAsync(oa[k], da[k], (size_t)n_targets * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return cuda_fail(e, "direct summation");
+  return ok();
+}
+
+int nbb_accel_octree(const nbb_octree_view *o, const uint32_t *idx, const double *mass, const double *x,
+                     const double *y, const double *z, double *ax, double *ay, double *az, double theta,
+                     double softening, double g, int particle_order, int on_device) {
+  // barnes_hut.cu:345-391 validation
+  if (!o || o->n_particles <= 0 || o->n_nodes <= 0)
+    return fail(NBB_ERR_LOGIC, "Octree is not valid for Barnes-Hut traversal");
+  if (!o->children || !o->parent || !o->first || !o->count)
+    return fail(NBB_ERR_LOGIC, "Octree topology arrays required for traversal are not allocated");
+  if (!o->mass || !o->comx || !o->comy || !o->comz) return fail(NBB_ERR_LOGIC, "Octree physical data is not allocated");
+  if (!o->cx || !o->cy || !o->cz || !o->half) return fail(NBB_ERR_LOGIC, "Octree geometry is not allocated");
+  if (!idx || !mass || !x || !y || !z)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut particle arrays must not be null");
+  if (!ax || !ay || !az) return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut acceleration arrays must not be null");
+  if (!finite_nonneg(theta)) return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut theta must be finite and non-negative");
+  if (!finite_nonneg(softening))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Barnes-Hut softening must be finite and non-negative");
+  if (!std::isfinite(g) || g <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Gravitational constant must be finite and positive");
+  if (particle_order != 0 && particle_order != 1) return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown Barnes-Hut particle order");
+  Allocation al;
+  cudaStream_t s = nullptr;
+  NBB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  const size_t M = (size_t)o->n_nodes, N = (size_t)o->n_particles;
+  RefOctree d{};
+  d.n_nodes = o->n_nodes;
+  d.n_particles = o->n_particles;
+  const bool dev = on_device != 0;
+  cudaError_t e = stage_in(o->children, 8 * M, dev, al, d.children, s);
+  if (e == cudaSuccess) e = stage_in(o->parent, M, dev, al, d.parent, s);
+  if (e == cudaSuccess) e = stage_in(o->first, M, dev, al, d.first, s);
+  if (e == cudaSuccess) e = stage_in(o->count, M, dev, al, d.count, s);
+  if (e == cudaSuccess) e = stage_in(o->mass, M, dev, al, d.mass, s);
+  if (e == cudaSuccess) e = stage_in(o->comx, M, dev, al, d.comx, s);
+  if (e == cudaSuccess) e = stage_in(o->comy, M, dev, al, d.comy, s);
+  if (e == cudaSuccess) e = stage_in(o->comz, M, dev, al, d.comz, s);
+  if (e == cudaSuccess) e = stage_in(o->cx, M, dev, al, d.cx, s);
+  if (e == cudaSuccess) e = stage_in(o->cy, M, dev, al, d.cy, s);
+  if (e == cudaSuccess) e = stage_in(o->cz, M, dev, al, d.cz, s);
+  if (e == cudaSuccess) e = stage_in(o->half, M, dev, al, d.half, s);
+  const uint32_t *di = nullptr;
+  const double *dm = nullptr, *dx = nullptr, *dy = nullptr, *dz = nullptr;
+  if (e == cudaSuccess) e = stage_in(idx, N, dev, al, di, s);
+  if (e == cudaSuccess) e = stage_in(mass, N, dev, al, dm, s);
+  if (e == cudaSuccess) e = stage_in(x, N, dev, al, dx, s);
+  if (e == cudaSuccess) e = stage_in(y, N, dev, al, dy, s);
+  if (e == cudaSuccess) e = stage_in(z, N, dev, al, dz, s);
+  double *oa[3] = {ax, ay, az};
+  double *da[3] = {ax, ay, az};
+  for (int k = 0; k < 3 && e == cudaSuccess && !dev; ++k) e = al.get(da[k], N);
+  int *derr = nullptr;
+  if (e == cudaSuccess) e = al.get(derr, 1);
+  if (e == cudaSuccess) e = cudaMemsetAsync(derr, 0, sizeof(int), s);
+  if (e == cudaSuccess)
+    e = launch_ref_octree_traversal(d, di, dm, dx, dy, dz, da[0], da[1], da[2], theta, softening, g,
+                                    particle_order, derr, s);
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, s);
+  for (int k = 0; k < 3 && e == cudaSuccess && !dev; ++k)
+    e = cudaMemcpyAsync(oa[k], da[k], N * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return cuda_fail(e, "computeBarnesHutAccelerationKernel execution");
+  if (herr) return fail(NBB_ERR_DEVICE, device_message(kStageTraversal, herr), kStageTraversal * 100 + herr);
+  return ok();
+}
+
+int nbb_kick_drift(double *x, double *y, double *z, double *vx, double *vy, double *vz, const double *ax,
+                   const double *ay, const double *az, size_t n, double dt, void *stream) {
+  // integrator.cu:115-132
+  if (!std::isfinite(dt) || dt <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog timestep must be finite and positive");
+  if (n == 0) return ok();
+  if (!x || !y || !z) return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog position arrays must not be null");
+  if (!vx || !vy || !vz) return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog velocity arrays must not be null");
+  if (!ax || !ay || !az) return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog acceleration arrays must not be null");
+  cudaStream_t s = (cudaStream_t)stream;
+  NBB_CUDA(launch_kick_drift(x, y, z, vx, vy, vz, ax, ay, az, n, dt, s), "leapfrogKickDriftKernel launch");
+  NBB_CUDA(cudaStreamSynchronize(s), "leapfrogKickDriftKernel execution");
+  return ok();
+}
+
+int nbb_kick(double *vx, double *vy, double *vz, const double *ax, const double *ay, const double *az, size_t n,
+             double dt, void *stream) {
+  // integrator.cu:135-151
+  if (!std::isfinite(dt) || dt <= 0.0)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog timestep must be finite and positive");
+  if (n == 0) return ok();
+  if (!vx || !vy || !vz) return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog velocity arrays must not be null");
+  if (!ax || !ay || !az) return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog acceleration arrays must not be null");
+  cudaStream_t s = (cudaStream_t)stream;
+  NBB_CUDA(launch_kick(vx, vy, vz, ax, ay, az, n, dt, s), "leapfrogKickKernel launch");
+  NBB_CUDA(cudaStreamSynchronize(s), "leapfrogKickKernel execution");
+  return ok();
+}
+
+int nbb_octree_from_keys(const uint32_t *sorted_keys, int n, nbb_tree_export *out) {
+  if (n <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "buildMortonLeafGroups requires nParticles >= 1");
+  if (!sorted_keys || !out) return fail(NBB_ERR_INVALID_ARGUMENT, "d_sortedKeys must not be null");
+  Scratch sc;
+  NBB_CUDA(cudaStreamCreateWithFlags(&sc.s, cudaStreamNonBlocking), "create stream");
+  NBB_CUDA(alloc_workspace(sc.ws, sc.al, n, false), "allocate workspace");
+  uint32_t *dk = nullptr;
+  NBB_CUDA(sc.al.get(dk, (size_t)n), "allocate keys");
+  NBB_CUDA(cudaMemcpyAsync(dk, sorted_keys, (size_t)n * 4, cudaMemcpyHostToDevice, sc.s), "copy keys");
+  NBB_CUDA(launch_step_reset(sc.ws, sc.s), "reset");
+  NBB_CUDA(launch_groups_from_keys(sc.ws, dk, sc.s), "buildMortonLeafGroups");
+  NBB_CUDA(launch_topology(sc.ws, sc.s), "octree topology");
+  const int st = check_device(sc.ws, sc.s);
+  if (st) return st;
+  return export_workspace(sc.ws, out, sc.s, false);
+}
+
+int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right, int *rfirst, int *rlast, int *plen,
+                   int *parent) {
+  if (n <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "buildTree requires N >= 1");
+  if (!keys) return fail(NBB_ERR_INVALID_ARGUMENT, "d_sortedKeys must not be null");
+  Allocation al;
+  cudaStream_t s = nullptr;
+  NBB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  uint32_t *dk = nullptr;
+  int *dl = nullptr, *dr = nullptr, *df = nullptr, *dla = nullptr, *dp = nullptr, *dpar = nullptr;
+  const size_t ni = n > 1 ? (size_t)(n - 1) : 1;
+  cudaError_t e = al.get(dk, (size_t)n);
+  if (e == cudaSuccess) e = al.get(dl, ni);
+  if (e == cudaSuccess) e = al.get(dr, ni);
+  if (e == cudaSuccess) e = al.get(df, ni);
+  if (e == cudaSuccess) e = al.get(dla, ni);
+  if (e == cudaSuccess) e = al.get(dp, ni);
+  if (e == cudaSuccess) e = al.get(dpar, (size_t)(2 * n - 1));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dk, keys, (size_t)n * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = launch_radix_tree_only(dk, n, dl, dr, df, dla, dp, dpar, s);
+  const size_t ib = (size_t)(n - 1) * sizeof(int);
+  if (n > 1) {
+    if (e == cudaSuccess && left) e = cudaMemcpyAsync(left, dl, ib, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && right) e = cudaMemcpyAsync(right, dr, ib, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && rfirst) e = cudaMemcpyAsync(rfirst, df, ib, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && rlast) e = cudaMemcpyAsync(rlast, dla, ib, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && plen) e = cudaMemcpyAsync(plen, dp, ib, cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess && parent)
+    e = cudaMemcpyAsync(parent, dpar, (size_t)(2 * n - 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return cuda_fail(e, "buildTreeKernel execution");
+  return ok();
+}
+
+}  // extern "C"

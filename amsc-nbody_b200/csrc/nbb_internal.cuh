@@ -1,0 +1,238 @@
+// nbb_internal.cuh -- device workspace, error words and small device helpers
+// shared by the build, traversal and C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace nbb {
+
+// src/radix_to_octree.hpp:10-19
+constexpr int kDims = 3;
+constexpr int kSpatialBits = 30;
+constexpr int kPaddingBits = 2;
+constexpr int kMaxLevel = 10;
+constexpr uint32_t kSpatialMask = 0x3FFFFFFFu;
+
+// Device error word: stage * 100 + code.  Codes 1..8 are the reference's own
+// device error codes of that stage; the rest are this library's.
+enum Stage : int {
+  kStageBbox = 1,       // code 1 non-finite position, 2 invalid box
+  kStageSort = 2,       // code 99 bounded look-back wait gave up
+  kStageGroups = 3,     // code 99 bounded look-back wait gave up
+  kStagePlan = 4,       // radix_to_octree.cu:102-121 codes 1..4; 90 overflow
+  kStageOctree = 5,     // octree_builder.cu:206-234 codes 1..7
+  kStageGeometry = 6,   // octree_geometry.cu:21-34 codes 1..2
+  kStagePhysics = 7,    // octree_physics.cu:190-218 codes 1..7
+  kStageTraversal = 8,  // barnes_hut.cu:41-72 codes 1..8
+  kStageLayout = 9      // code 1 inconsistent preorder walk
+};
+constexpr int kCodeTimeout = 99;
+constexpr int kCodeOverflow = 90;
+
+// Per-workspace device scalars; one block reset at the start of each step.
+struct DevScalars {
+  unsigned long long bb_min[3];  // order-preserving encoded extrema
+  unsigned long long bb_max[3];
+  double box[4];                 // centre x, y, z, side (Bbox layout)
+  int nonfinite;
+  int n_groups;                  // G
+  int n_nodes;                   // M
+  int error;                     // sticky first error (not reset per step)
+  unsigned int ticket_bbox;
+  unsigned int ticket_encode;
+  unsigned int tile_counter[8];  // dynamic tile ids of single-pass kernels
+  unsigned int work_counter;     // traversal work queue
+  unsigned int stack_overflow;   // mixed traversal nodes accepted on overflow
+  unsigned long long interactions;
+  unsigned long long mac_tests;
+};
+
+// Sort tiling (onesweep LSD radix sort of packed (key << 32 | index)).
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs
+constexpr int kSortPasses = 4;                        // 8-bit digits, bits 32..63
+
+// Single-pass scan tiling.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Everything a spatial rebuild and a traversal touch, sized for capacity n.
+struct Workspace {
+  int n = 0;            // particle count
+  int cap_nodes = 0;    // octree node capacity (sum over levels of min(8^L, n))
+  int num_sms = 0;
+  int fp64_grid = 0;    // persistent traversal grids (blocks)
+  int mixed_grid = 0;
+
+  // particle state, original order (SoA, FP64)
+  double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  double *ax = nullptr, *ay = nullptr, *az = nullptr;
+  uint8_t *type = nullptr;
+
+  DevScalars *sc = nullptr;
+
+  // sort
+  unsigned long long *pairs_a = nullptr, *pairs_b = nullptr;  // n each
+  uint32_t *digit_hist = nullptr;    // kSortPasses * 256 (counts -> offsets)
+  uint32_t *sort_status = nullptr;   // kSortPasses * tiles * 256
+  int sort_tiles = 0;
+  unsigned long long *scan_status = nullptr;  // 2 * scan tiles (groups, plan)
+  int scan_tiles_n = 0;   // tiles over n
+  int scan_tiles_r = 0;   // tiles over 2n-1
+
+  // Morton keys / permutation (reference MortonKeys layout)
+  uint32_t *keys = nullptr, *idx = nullptr;
+  double4 *pm4 = nullptr;  // Morton-ordered particles {x, y, z, m}
+
+  // leaf groups (MortonLeafGroups)
+  uint32_t *uniq = nullptr;
+  int *gfirst = nullptr, *gcount = nullptr, *glast = nullptr;
+
+  // radix tree (Tree): internal n-1, all nodes 2n-1
+  int *left = nullptr, *right = nullptr, *rfirst = nullptr, *rlast = nullptr,
+      *plen = nullptr, *rparent = nullptr;
+
+  // plan (RadixToOctreePlan), 2n-1
+  int *plevel = nullptr, *pcount = nullptr, *poffset = nullptr;
+
+  // octree, reference numbering (Octree), cap_nodes
+  int *children = nullptr, *oparent = nullptr, *olevel = nullptr;
+  uint32_t *oprefix = nullptr;
+  int *ofirst = nullptr, *ocount = nullptr, *child_count = nullptr,
+      *pending = nullptr;
+  double *cx = nullptr, *cy = nullptr, *cz = nullptr, *half = nullptr;
+  double *mass = nullptr, *comx = nullptr, *comy = nullptr, *comz = nullptr;
+  int *subtree = nullptr, *preoff = nullptr;
+
+  // traversal layout: depth-first preorder, children visited octant 7 -> 0
+  double4 *node_a = nullptr;  // com x, y, z, mass
+  double4 *node_b = nullptr;  // centre x, y, z, half size
+  double4 *node_c = nullptr;  // crit, crit^2 lower/upper band, unused
+  int4 *node_meta = nullptr;  // skip, first particle, particle count, nchild
+  int *node_kids = nullptr;   // 8 per node, preorder ids in visit order
+};
+
+// ------------------------------------------------------------ helpers ---
+
+__device__ __forceinline__ void record_error(DevScalars *sc, int stage,
+                                             int code) {
+  atomicCAS(&sc->error, 0, stage * 100 + code);
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(
+    const unsigned long long *p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p,
+                                               unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Order-preserving map of a double onto unsigned 64-bit integers.
+__device__ __forceinline__ unsigned long long order_bits(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double order_value(unsigned long long k) {
+  const unsigned long long b =
+      (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// Spin limit of every bounded device wait (look-back).  Far above any wait
+// that a live predecessor can cause; reaching it records kCodeTimeout.
+constexpr int kSpinLimit = 1 << 22;
+
+}  // namespace nbb
+
+// Host-side entry points of the build and traversal translation units.
+namespace nbb {
+
+struct TraversalParams {
+  double theta = 0.5;
+  double soft = 0.0;
+  double g = 1.0;
+  double half_dt = 0.0;  // second half kick fused into the epilogue when kick
+  int kick = 0;
+  int precision = 0;     // 0 FP64 plain, 1 mixed
+  int group_size = 32;
+};
+
+// Launch-count bookkeeping (kernels launched by this library).
+void count_launches(uint64_t k);
+uint64_t launch_count();
+
+// Reset per-step device scalars (sticky error untouched) and status arrays.
+cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s);
+// Kick-drift (optional) fused with the global bounding-box reduction.
+cudaError_t launch_kd_bbox(Workspace &ws, double dt, int do_kd, cudaStream_t s);
+// Morton encode + digit histograms, onesweep sort, groups + gather.
+cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s);
+// Karras tree, plan + scan, octree materialisation, geometry, physics,
+// preorder layout.
+cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s);
+// Traversal (+ optional fused second half kick).
+cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p,
+                             cudaStream_t s);
+// Diagnostic SIMT FMA throughput, TFLOP/s (precision 0 FP64, 1 FP32).
+cudaError_t measure_fma_tflops(int precision, double *tflops);
+// Plain kick / kick-drift over n particles.
+cudaError_t launch_kick(double *vx, double *vy, double *vz, const double *ax,
+                        const double *ay, const double *az, size_t n,
+                        double dt, cudaStream_t s);
+cudaError_t launch_kick_drift(double *x, double *y, double *z, double *vx,
+                              double *vy, double *vz, const double *ax,
+                              const double *ay, const double *az, size_t n,
+                              double dt, cudaStream_t s);
+// FP64 direct sum for a target list.
+cudaError_t launch_direct(size_t n, const double *m, const double *x,
+                          const double *y, const double *z, int n_targets,
+                          const int *targets, double g, double soft,
+                          double *ax, double *ay, double *az, cudaStream_t s);
+// Traversal on a caller octree in the reference numbering (FP64 plain).
+struct RefOctree {
+  int n_nodes, n_particles;
+  const int *children, *parent, *first, *count;
+  const double *mass, *comx, *comy, *comz, *cx, *cy, *cz, *half;
+};
+cudaError_t launch_ref_octree_traversal(const RefOctree &o, const uint32_t *idx,
+                                        const double *m, const double *x,
+                                        const double *y, const double *z,
+                                        double *ax, double *ay, double *az,
+                                        double theta, double soft, double g,
+                                        int morton_order, int *err,
+                                        cudaStream_t s);
+// Karras tree alone over caller keys (any 32-bit keys, duplicates allowed).
+cudaError_t launch_radix_tree_only(const uint32_t *keys, int n, int *left,
+                                   int *right, int *rfirst, int *rlast,
+                                   int *plen, int *parent, cudaStream_t s);
+// Leaf groups from caller sorted keys (no particles): fills uniq / gfirst /
+// gcount / glast and n_groups.
+cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys,
+                                    cudaStream_t s);
+// Topology stages only (Karras .. materialise) for caller keys.
+cudaError_t launch_topology(Workspace &ws, cudaStream_t s);
+
+}  // namespace nbb

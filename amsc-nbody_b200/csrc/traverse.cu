@@ -1,0 +1,739 @@
+// traverse.cu -- Barnes-Hut force evaluation on sm_100a.
+//
+//  traverse_fp64_kernel   plain form of barnes_hut.cu:184-342 (paths relative
+//                         to the sytrams/AMSC-Nbody project root): per-target
+//                         acceptance test and interaction order identical to
+//                         the reference, FP64 throughout.
+//  traverse_mixed_kernel  mixed form: warp-group acceptance test, shared
+//                         interaction lists evaluated in FP32.
+//  direct_kernel          FP64 direct summation (theta-error oracle).
+//  ref_octree_kernel      traversal of a caller octree in the reference's own
+//                         node numbering (function-level API).
+//  kick / kick_drift      integrator.cu:57-112.
+#include "nbb_internal.cuh"
+
+#include <climits>
+#include <cmath>
+
+namespace nbb {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// barnes_hut.cu:76-100: G m (d^2 + eps^2)^-3/2 d, accumulated with the
+// reference's operation order.  Returns false on a singular interaction.
+__device__ __forceinline__ bool point_mass_fp64(double dx, double dy, double dz, double d2,
+                                                double m, double g, double soft2, double &ax,
+                                                double &ay, double &az) {
+  const double r2 = __dadd_rn(d2, soft2);
+  if (r2 <= 0.0) return false;
+  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
+  const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
+  const double f = __dmul_rn(__dmul_rn(g, m), inv3);
+  ax = __fma_rn(f, dx, ax);
+  ay = __fma_rn(f, dy, ay);
+  az = __fma_rn(f, dz, az);
+  return true;
+}
+
+__device__ __forceinline__ double sqdist(double dx, double dy, double dz) {
+  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Plain FP64 traversal, one warp per 32 Morton-consecutive targets.
+//
+// The tree is laid out in depth-first preorder with children visited octant
+// 7 -> 0, so the reference's per-thread stackless walk (barnes_hut.cu:110-182)
+// becomes: a target opened at node i continues at i + 1, a target done with
+// node i (accepted, zero mass, or a leaf) continues at skip(i).  Each lane
+// keeps its own resume index and the warp always visits the smallest one, so
+// every lane sees exactly its own node sequence -- the reference's
+// interaction set in the reference's order -- while node records are fetched
+// once per warp (broadcast loads) instead of once per thread.
+__global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, TraversalParams p) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int lane = threadIdx.x & 31;
+  const int n = ws.n;
+  const int m = sc->n_nodes;
+  const int n_groups = (n + 31) >> 5;
+  const double soft2 = __dmul_rn(p.soft, p.soft);
+  const double g = p.g;
+  long long inter = 0, tests = 0;
+  bool singular = false;
+  while (true) {
+    int grp = 0;
+    if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
+    grp = __shfl_sync(kFull, grp, 0);
+    if (grp >= n_groups) break;
+    const int s = grp * 32 + lane;
+    const bool valid = s < n;
+    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (valid) t = ws.pm4[s];
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    int resume = valid ? 0 : INT_MAX;
+    int node = __reduce_min_sync(kFull, resume);
+    while (node < m) {
+      if (resume == node) {
+        const int4 meta = ws.node_meta[node];
+        if (meta.z > 0) {
+          // occupied leaf: exact sum over its particles, self excluded
+          // (barnes_hut.cu:226-277)
+          for (int k = 0; k < meta.z; ++k) {
+            const int sp = meta.y + k;
+            if (sp == s) continue;
+            const double4 q = ws.pm4[sp];
+            if (q.w == 0.0) continue;
+            const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
+            singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
+            ++inter;
+          }
+          resume = meta.x;
+        } else {
+          const double4 a = ws.node_a[node];
+          if (a.w == 0.0) {
+            resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
+          } else {
+            const double dx = __dsub_rn(a.x, t.x), dy = __dsub_rn(a.y, t.y), dz = __dsub_rn(a.z, t.z);
+            const double d2 = sqdist(dx, dy, dz);
+            const double4 c = ws.node_c[node];
+            // sqrt(d2) > crit, decided on d2 vs crit^2 outside a 2^-44 band
+            bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
+            ++tests;
+            if (accept) {
+              const double4 b = ws.node_b[node];
+              const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w &&
+                                    fabs(__dsub_rn(t.y, b.y)) <= b.w &&
+                                    fabs(__dsub_rn(t.z, b.z)) <= b.w;
+              accept = !contains && d2 > 0.0;
+            }
+            if (accept) {
+              singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
+              ++inter;
+              resume = meta.x;
+            } else {
+              resume = node + 1;
+            }
+          }
+        }
+      }
+      // a lane's resume index always moves forward (skip > node); this keeps
+      // the walk finite whatever the node records hold
+      if (resume <= node) resume = node + 1;
+      node = __reduce_min_sync(kFull, resume);
+    }
+    if (valid) {
+      const uint32_t ti = ws.idx[s];
+      ws.ax[ti] = ax;
+      ws.ay[ti] = ay;
+      ws.az[ti] = az;
+      if (p.kick) {
+        // second half kick, integrator.cu:92-112
+        ws.vx[ti] = __fma_rn(p.half_dt, ax, ws.vx[ti]);
+        ws.vy[ti] = __fma_rn(p.half_dt, ay, ws.vy[ti]);
+        ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
+      }
+    }
+  }
+  if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
+  inter = warp_sum_ll(inter);
+  tests = warp_sum_ll(tests);
+  if (lane == 0) {
+    atomicAdd(&sc->interactions, (unsigned long long)inter);
+    atomicAdd(&sc->mac_tests, (unsigned long long)tests);
+  }
+}
+
+// ------------------------------------------------------------ mixed ----
+
+constexpr int kMixedWarps = 4;
+constexpr int kStackCap = 1536;
+constexpr int kListCap = 64;
+
+struct MixedShared {
+  int stack[kMixedWarps][kStackCap];
+  float4 list[kMixedWarps][kListCap];
+  int src[kMixedWarps][kListCap];
+};
+
+// Evaluate `count` list entries for this lane's target: FP32 offsets, rsqrtf
+// plus one Newton step, plain FP32 partial sum over the batch, then one
+// Kahan-compensated addition of the batch partial into the running sum.
+// Returns true when a non-self entry coincides with the target at zero
+// softening (the reference's singular-interaction error).
+__device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, int count, int self,
+                                           float tx, float ty, float tz, float eps2, float3 &sum,
+                                           float3 &comp) {
+  float px = 0.f, py = 0.f, pz = 0.f;
+  bool singular = false;
+#pragma unroll 8
+  for (int j = 0; j < count; ++j) {
+    const float4 e = list[j];
+    const int sidx = src[j];
+    const float dx = e.x - tx, dy = e.y - ty, dz = e.z - tz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    float r = rsqrtf(r2);
+    r = r * fmaf(-0.5f * r2, r * r, 1.5f);
+    const bool other = sidx != self;
+    const bool use = other && (r2 > 0.f);
+    singular |= other && !(r2 > 0.f) && e.w != 0.f;
+    const float f = use ? e.w * (r * r * r) : 0.f;
+    px = fmaf(f, dx, px);
+    py = fmaf(f, dy, py);
+    pz = fmaf(f, dz, pz);
+  }
+  float y, t;
+  y = px - comp.x; t = sum.x + y; comp.x = (t - sum.x) - y; sum.x = t;
+  y = py - comp.y; t = sum.y + y; comp.y = (t - sum.y) - y; sum.y = t;
+  y = pz - comp.z; t = sum.z + y; comp.z = (t - sum.z) - y; sum.z = t;
+  return singular;
+}
+
+// Evaluate the first 32 list entries and shift the remainder down.
+__device__ __forceinline__ void flush32(float4 *list, int *src, int &ls, int self, bool valid,
+                                        float tx, float ty, float tz, float eps2, float3 &sum,
+                                        float3 &comp, long long &inter, bool &singular) {
+  const int lane = threadIdx.x & 31;
+  const bool sg = eval_batch(list, src, 32, self, tx, ty, tz, eps2, sum, comp);
+  if (valid) {
+    inter += 32;
+    singular |= sg;
+  }
+  __syncwarp();
+  if (lane < ls - 32) {
+    list[lane] = list[32 + lane];
+    src[lane] = src[32 + lane];
+  }
+  ls -= 32;
+  __syncwarp();
+}
+
+// Mixed-precision traversal, one warp per group of 32 Morton-consecutive
+// targets.  The group's bounding box (FP64) replaces the target in the
+// reference's acceptance test: a node is accepted for the whole group when
+// the box does not touch the cell and the box-to-centre-of-mass distance
+// exceeds crit = side/theta + |com - centre|, which implies acceptance for
+// every target in the box.  Nodes are examined 32 at a time (one per lane)
+// from a warp-private stack in shared memory; accepted nodes and the
+// particles of reached leaves go to a shared interaction list as FP32
+// offsets from the group centre (formed in FP64, then rounded) and are
+// evaluated by all 32 lanes in batches of 32.
+__global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Workspace ws,
+                                                                          TraversalParams p) {
+  __shared__ MixedShared sh;
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  int *stack = sh.stack[wid];
+  float4 *list = sh.list[wid];
+  int *src = sh.src[wid];
+  const int n = ws.n;
+  const int m = sc->n_nodes;
+  const int n_groups = (n + 31) >> 5;
+  const float eps2 = (float)(p.soft * p.soft);
+  const unsigned lt = lanemask_lt();
+  long long inter = 0, tests = 0;
+  unsigned overflow = 0;
+  bool singular = false;
+  while (true) {
+    int grp = 0;
+    if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
+    grp = __shfl_sync(kFull, grp, 0);
+    if (grp >= n_groups) break;
+    const int s = grp * 32 + lane;
+    const bool valid = s < n;
+    const double4 t = ws.pm4[valid ? s : grp * 32];
+    double lo[3] = {t.x, t.y, t.z}, hi[3] = {t.x, t.y, t.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[a] = fmin(lo[a], __shfl_xor_sync(kFull, lo[a], o));
+        hi[a] = fmax(hi[a], __shfl_xor_sync(kFull, hi[a], o));
+      }
+    }
+    const double gcx = 0.5 * (lo[0] + hi[0]), gcy = 0.5 * (lo[1] + hi[1]),
+                 gcz = 0.5 * (lo[2] + hi[2]);
+    const float tx = (float)(t.x - gcx), ty = (float)(t.y - gcy), tz = (float)(t.z - gcz);
+    float3 sum = make_float3(0.f, 0.f, 0.f), comp = make_float3(0.f, 0.f, 0.f);
+    int ls = 0;
+    if (lane == 0) stack[0] = 0;
+    int sp = (m > 0) ? 1 : 0;
+    __syncwarp();
+    while (sp > 0) {
+      int k = sp < 32 ? sp : 32;
+      const int room = (kStackCap - sp) / 7;
+      if (k > room) k = room > 0 ? room : 1;
+      const int node = (lane < k) ? stack[sp - k + lane] : -1;
+      sp -= k;
+      __syncwarp();
+      int cat = 0;  // 0 nothing, 1 accepted cell, 2 leaf, 3 open
+      int4 meta = make_int4(0, 0, 0, 0);
+      double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (node >= 0) {
+        meta = ws.node_meta[node];
+        if (meta.z > 0) {
+          cat = 2;
+        } else {
+          a = ws.node_a[node];
+          if (a.w != 0.0) {
+            const double4 b = ws.node_b[node];
+            const double crit = ws.node_c[node].x;
+            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
+            bool overlap = true;
+            double d2 = 0.0;
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+              overlap = overlap && hi[ax] >= cen[ax] - b.w && lo[ax] <= cen[ax] + b.w;
+              const double e = fmax(0.0, fmax(lo[ax] - com[ax], com[ax] - hi[ax]));
+              d2 = fma(e, e, d2);
+            }
+            ++tests;
+            cat = (!overlap && sqrt(d2) > crit) ? 1 : 3;
+          }
+        }
+      }
+      // opened nodes push their children; a push that would not fit the
+      // stack accepts the node instead (bounded walk, counted)
+      int nch = (cat == 3) ? meta.w : 0;
+      int incl = nch;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int excl = incl - nch;
+      if (nch > 0 && sp + incl > kStackCap) {
+        cat = 1;
+        nch = 0;
+        ++overflow;
+      }
+      int pushed = (nch > 0) ? incl : 0;
+      for (int o = 16; o > 0; o >>= 1) pushed = max(pushed, __shfl_xor_sync(kFull, pushed, o));
+      if (nch > 0) {
+        // children always follow their parent in preorder; anything else is
+        // dropped so the walk stays finite
+        const int *kids = ws.node_kids + (size_t)node * 8;
+        for (int j = 0; j < nch; ++j) {
+          const int c = kids[j];
+          stack[sp + excl + j] = (c > node && c < m) ? c : -1;
+        }
+      }
+      sp += pushed;
+      // accepted cells -> interaction list
+      const unsigned cm = __ballot_sync(kFull, cat == 1);
+      if (cat == 1) {
+        const int pos = ls + __popc(cm & lt);
+        list[pos] = make_float4((float)(a.x - gcx), (float)(a.y - gcy), (float)(a.z - gcz), (float)a.w);
+        src[pos] = -1;
+      }
+      ls += __popc(cm);
+      __syncwarp();
+      while (ls >= 32) flush32(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+      // reached leaves -> their particles, 32 at a time
+      unsigned lm = __ballot_sync(kFull, cat == 2);
+      while (lm) {
+        const int l = __ffs(lm) - 1;
+        lm &= lm - 1;
+        const int first = __shfl_sync(kFull, meta.y, l);
+        const int cnt = __shfl_sync(kFull, meta.z, l);
+        for (int b0 = 0; b0 < cnt; b0 += 32) {
+          const int j = b0 + lane;
+          if (j < cnt) {
+            const double4 q = ws.pm4[first + j];
+            list[ls + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+            src[ls + lane] = first + j;
+          }
+          ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
+          __syncwarp();
+          if (ls >= 32) flush32(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+        }
+      }
+    }
+    if (ls > 0) {
+      const bool sg = eval_batch(list, src, ls, s, tx, ty, tz, eps2, sum, comp);
+      if (valid) {
+        inter += ls;
+        singular |= sg;
+      }
+    }
+    __syncwarp();
+    if (valid) {
+      const double ax = p.g * ((double)sum.x - (double)comp.x);
+      const double ay = p.g * ((double)sum.y - (double)comp.y);
+      const double az = p.g * ((double)sum.z - (double)comp.z);
+      const uint32_t ti = ws.idx[s];
+      ws.ax[ti] = ax;
+      ws.ay[ti] = ay;
+      ws.az[ti] = az;
+      if (p.kick) {
+        ws.vx[ti] = __fma_rn(p.half_dt, ax, ws.vx[ti]);
+        ws.vy[ti] = __fma_rn(p.half_dt, ay, ws.vy[ti]);
+        ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
+      }
+    }
+  }
+  if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
+  inter = warp_sum_ll(inter);
+  tests = warp_sum_ll(tests);
+  unsigned ov = overflow;
+  for (int o = 16; o > 0; o >>= 1) ov += __shfl_xor_sync(kFull, ov, o);
+  if (lane == 0) {
+    atomicAdd(&sc->interactions, (unsigned long long)inter);
+    atomicAdd(&sc->mac_tests, (unsigned long long)tests);
+    if (ov) atomicAdd(&sc->stack_overflow, ov);
+  }
+}
+
+// ------------------------------------------------------------ direct ----
+
+constexpr int kDirectThreads = 128;
+
+// barnes_hut_accuracy_test.cu:101-172: each thread sums every other particle
+// in index order; sources are staged through shared memory in tiles.
+__global__ void __launch_bounds__(kDirectThreads)
+    direct_kernel(int n, const double *__restrict__ m, const double *__restrict__ x,
+                  const double *__restrict__ y, const double *__restrict__ z, int n_targets,
+                  const int *__restrict__ targets, double g, double soft2, double *ax, double *ay,
+                  double *az) {
+  __shared__ double4 tile[kDirectThreads];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int t = (k < n_targets) ? (targets ? targets[k] : k) : 0;
+  const bool active = k < n_targets && t >= 0 && t < n;
+  if (!active) t = 0;
+  const double tx = active ? x[t] : 0.0, ty = active ? y[t] : 0.0, tz = active ? z[t] : 0.0;
+  double rx = 0.0, ry = 0.0, rz = 0.0;
+  for (int base = 0; base < n; base += kDirectThreads) {
+    const int j = base + threadIdx.x;
+    tile[threadIdx.x] = (j < n) ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
+    __syncthreads();
+    const int lim = (n - base < kDirectThreads) ? n - base : kDirectThreads;
+    if (active) {
+      for (int q = 0; q < lim; ++q) {
+        if (base + q == t) continue;
+        const double4 s = tile[q];
+        const double dx = __dsub_rn(s.x, tx), dy = __dsub_rn(s.y, ty), dz = __dsub_rn(s.z, tz);
+        const double d2 = __dadd_rn(sqdist(dx, dy, dz), soft2);
+        const double inv = __ddiv_rn(1.0, __dsqrt_rn(d2));
+        const double f = __dmul_rn(__dmul_rn(g, s.w), __dmul_rn(__dmul_rn(inv, inv), inv));
+        rx = __fma_rn(f, dx, rx);
+        ry = __fma_rn(f, dy, ry);
+        rz = __fma_rn(f, dz, rz);
+      }
+    }
+    __syncthreads();
+  }
+  if (k < n_targets) {
+    ax[k] = active ? rx : NAN;
+    ay[k] = active ? ry : NAN;
+    az[k] = active ? rz : NAN;
+  }
+}
+
+// ------------------------------------------- reference-layout octree ----
+
+// barnes_hut.cu:110-182 on a caller octree in the reference numbering.
+__device__ int ref_first_child(const RefOctree &o, int node, int &err) {
+  for (int oc = 7; oc >= 0; --oc) {
+    const int c = o.children[node * 8 + oc];
+    if (c == -1) continue;
+    if (c <= 0 || c >= o.n_nodes) {
+      err = 1;
+      return -2;
+    }
+    return c;
+  }
+  err = 5;
+  return -2;
+}
+
+__device__ int ref_next(const RefOctree &o, int node, int &err) {
+  int climbs = 0;
+  while (node != 0) {
+    if (++climbs > o.n_nodes) {
+      err = 4;
+      return -2;
+    }
+    const int par = o.parent[node];
+    if (par < 0 || par >= o.n_nodes) {
+      err = 4;
+      return -2;
+    }
+    bool found = false;
+    for (int oc = 7; oc >= 0; --oc) {
+      const int c = o.children[par * 8 + oc];
+      if (c == -1) continue;
+      if (c <= 0 || c >= o.n_nodes) {
+        err = 1;
+        return -2;
+      }
+      if (found) return c;
+      if (c == node) found = true;
+    }
+    if (!found) {
+      err = 4;
+      return -2;
+    }
+    node = par;
+  }
+  return -1;
+}
+
+__global__ void ref_octree_kernel(RefOctree o, const uint32_t *idx, const double *pm,
+                                  const double *px, const double *py, const double *pz, double *ax,
+                                  double *ay, double *az, double theta, double soft2, double g,
+                                  int morton, int *err_out) {
+  const int st = blockIdx.x * blockDim.x + threadIdx.x;
+  if (st >= o.n_particles) return;
+  int err = 0;
+  const uint32_t tu = idx[st];
+  if (tu >= (uint32_t)o.n_particles) {
+    atomicCAS(err_out, 0, 3);
+    return;
+  }
+  const int target = (int)tu;
+  const int ti = morton ? st : target;
+  const double tx = px[ti], ty = py[ti], tz = pz[ti];
+  double rx = 0.0, ry = 0.0, rz = 0.0;
+  int node = 0;
+  long long visits = 0;
+  const long long max_visits = 2ll * o.n_nodes + 8;
+  while (node >= 0) {
+    if (++visits > max_visits) {  // a cyclic caller octree never ends
+      atomicCAS(err_out, 0, 4);
+      return;
+    }
+    const double h = o.half[node];
+    if (h <= 0.0) {
+      atomicCAS(err_out, 0, 8);
+      return;
+    }
+    const int cnt = o.count[node];
+    if (cnt > 0) {
+      for (int oc = 0; oc < 8; ++oc)
+        if (o.children[node * 8 + oc] != -1) {
+          atomicCAS(err_out, 0, 7);
+          return;
+        }
+      const int f = o.first[node];
+      if (f < 0 || cnt > o.n_particles || f > o.n_particles - cnt) {
+        atomicCAS(err_out, 0, 2);
+        return;
+      }
+      for (int k = 0; k < cnt; ++k) {
+        const int sp = f + k;
+        const uint32_t su = idx[sp];
+        if (su >= (uint32_t)o.n_particles) {
+          atomicCAS(err_out, 0, 3);
+          return;
+        }
+        if (su == tu) continue;
+        const int si = morton ? sp : (int)su;
+        if (pm[si] == 0.0) continue;
+        const double dx = __dsub_rn(px[si], tx), dy = __dsub_rn(py[si], ty), dz = __dsub_rn(pz[si], tz);
+        if (!point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), pm[si], g, soft2, rx, ry, rz)) {
+          atomicCAS(err_out, 0, 6);
+          return;
+        }
+      }
+      node = ref_next(o, node, err);
+      if (node == -2) {
+        atomicCAS(err_out, 0, err);
+        return;
+      }
+      continue;
+    }
+    const double nm = o.mass[node];
+    if (nm == 0.0) {
+      node = ref_next(o, node, err);
+      if (node == -2) {
+        atomicCAS(err_out, 0, err);
+        return;
+      }
+      continue;
+    }
+    const double dx = __dsub_rn(o.comx[node], tx), dy = __dsub_rn(o.comy[node], ty),
+                 dz = __dsub_rn(o.comz[node], tz);
+    const double d2 = sqdist(dx, dy, dz);
+    const bool contains = fabs(__dsub_rn(tx, o.cx[node])) <= h && fabs(__dsub_rn(ty, o.cy[node])) <= h &&
+                          fabs(__dsub_rn(tz, o.cz[node])) <= h;
+    bool accept = false;
+    if (!contains && d2 > 0.0 && theta > 0.0) {
+      const double ox = __dsub_rn(o.comx[node], o.cx[node]), oy = __dsub_rn(o.comy[node], o.cy[node]),
+                   oz = __dsub_rn(o.comz[node], o.cz[node]);
+      const double crit = __dadd_rn(__ddiv_rn(__dmul_rn(2.0, h), theta), __dsqrt_rn(sqdist(ox, oy, oz)));
+      accept = __dsqrt_rn(d2) > crit;
+    }
+    if (accept) {
+      if (!point_mass_fp64(dx, dy, dz, d2, nm, g, soft2, rx, ry, rz)) {
+        atomicCAS(err_out, 0, 6);
+        return;
+      }
+      node = ref_next(o, node, err);
+    } else {
+      node = ref_first_child(o, node, err);
+    }
+    if (node == -2) {
+      atomicCAS(err_out, 0, err);
+      return;
+    }
+  }
+  ax[target] = rx;
+  ay[target] = ry;
+  az[target] = rz;
+}
+
+// ---------------------------------------------------------- integrator --
+
+__global__ void kick_drift_kernel(double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                                  const double *ax, const double *ay, const double *az, size_t n,
+                                  double dt) {
+  const double hdt = 0.5 * dt;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double nvx = __fma_rn(hdt, ax[i], vx[i]);
+    const double nvy = __fma_rn(hdt, ay[i], vy[i]);
+    const double nvz = __fma_rn(hdt, az[i], vz[i]);
+    vx[i] = nvx;
+    vy[i] = nvy;
+    vz[i] = nvz;
+    x[i] = __fma_rn(dt, nvx, x[i]);
+    y[i] = __fma_rn(dt, nvy, y[i]);
+    z[i] = __fma_rn(dt, nvz, z[i]);
+  }
+}
+
+__global__ void kick_kernel(double *vx, double *vy, double *vz, const double *ax, const double *ay,
+                            const double *az, size_t n, double dt) {
+  const double hdt = 0.5 * dt;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    vx[i] = __fma_rn(hdt, ax[i], vx[i]);
+    vy[i] = __fma_rn(hdt, ay[i], vy[i]);
+    vz[i] = __fma_rn(hdt, az[i], vz[i]);
+  }
+}
+
+// Diagnostic: SIMT FMA throughput (8 independent chains per thread).
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T *out, int iters, T a, T b) {
+  T x0 = (T)threadIdx.x * (T)1e-3, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3;
+  T x4 = x0 + (T)4, x5 = x0 + (T)5, x6 = x0 + (T)6, x7 = x0 + (T)7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  const T s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (s == (T)-12345) out[threadIdx.x] = s;
+}
+
+inline int stream_grid(size_t n, int num_sms) {
+  size_t b = (n + 255) / 256;
+  const size_t cap = (size_t)(num_sms > 0 ? num_sms : 148) * 8;
+  if (b > cap) b = cap;
+  return b < 1 ? 1 : (int)b;
+}
+
+int device_sms() {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+}  // namespace
+
+// Persistent grids: as many resident blocks as the occupancy calculator
+// allows on every SM; warps then pull target groups from a work counter.
+cudaError_t configure_traversal(Workspace &ws) {
+  const int sms = ws.num_sms > 0 ? ws.num_sms : 148;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_fp64_kernel, 256, 0);
+  if (e != cudaSuccess) return e;
+  ws.fp64_grid = sms * (per_sm > 0 ? per_sm : 1);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel, kMixedWarps * 32, 0);
+  if (e != cudaSuccess) return e;
+  ws.mixed_grid = sms * (per_sm > 0 ? per_sm : 1);
+  return cudaSuccess;
+}
+
+cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p, cudaStream_t s) {
+  if (p.precision == 0)
+    traverse_fp64_kernel<<<ws.fp64_grid > 0 ? ws.fp64_grid : 148, 256, 0, s>>>(ws, p);
+  else
+    traverse_mixed_kernel<<<ws.mixed_grid > 0 ? ws.mixed_grid : 148, kMixedWarps * 32, 0, s>>>(ws, p);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t measure_fma_tflops(int precision, double *tflops) {
+  const int sms = device_sms();
+  const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+  void *out = nullptr;
+  cudaError_t e = cudaMalloc(&out, 256 * sizeof(double));
+  if (e != cudaSuccess) return e;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    cudaEventRecord(e0);
+    if (precision == 0)
+      fma_peak_kernel<double><<<blocks, threads>>>((double *)out, iters, 0.9999999, 1e-9);
+    else
+      fma_peak_kernel<float><<<blocks, threads>>>((float *)out, iters * 2, 0.9999f, 1e-6f);
+    cudaEventRecord(e1);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  count_launches(4);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (e != cudaSuccess) return e;
+  const double flops = 2.0 * 8.0 * (double)iters * (precision == 0 ? 1.0 : 2.0) * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return cudaSuccess;
+}
+
+cudaError_t launch_kick(double *vx, double *vy, double *vz, const double *ax, const double *ay,
+                        const double *az, size_t n, double dt, cudaStream_t s) {
+  kick_kernel<<<stream_grid(n, device_sms()), 256, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kick_drift(double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                              const double *ax, const double *ay, const double *az, size_t n,
+                              double dt, cudaStream_t s) {
+  kick_drift_kernel<<<stream_grid(n, device_sms()), 256, 0, s>>>(x, y, z, vx, vy, vz, ax, ay, az, n, dt);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct(size_t n, const double *m, const double *x, const double *y, const double *z,
+                          int n_targets, const int *targets, double g, double soft, double *ax,
+                          double *ay, double *az, cudaStream_t s) {
+  const int blocks = (n_targets + kDirectThreads - 1) / kDirectThreads;
+  direct_kernel<<<blocks > 0 ? blocks : 1, kDirectThreads, 0, s>>>((int)n, m, x, y, z, n_targets, targets,
+                                                                  g, soft * soft, ax, ay, az);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ref_octree_traversal(const RefOctree &o, const uint32_t *idx, const double *m,
+                                        const double *x, const double *y, const double *z, double *ax,
+                                        double *ay, double *az, double theta, double soft, double g,
+                                        int morton_order, int *err, cudaStream_t s) {
+  const int blocks = (o.n_particles + 127) / 128;
+  ref_octree_kernel<<<blocks > 0 ? blocks : 1, 128, 0, s>>>(o, idx, m, x, y, z, ax, ay, az, theta,
+                                                            soft * soft, g, morton_order, err);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+}  // namespace nbb

@@ -1,0 +1,439 @@
+"""Benchmark of the Barnes-Hut step: steps/s at N=2^20, theta=0.5.
+
+Workload: Plummer sphere (G=1, total mass 1, a=1, r<10a, AHW velocities,
+centre of mass removed), N = 2^20, theta = 0.5, eps = 0.01, dt = 1e-3,
+synthetic and seeded.  One step = leapfrog KD + full spatial rebuild + force
+evaluation + K, replayed from a CUDA graph.  ``value`` is the steps/s of the
+mixed-precision form summed over all GPUs; the FP64 plain form is measured
+on the same GPU in the same run (``plain_fp64``), and the mixed form's force
+error against FP64 direct summation on 4096 seeded targets is reported
+(``force_error``): the headline is valid when its RMS relative error is
+<= 1e-3.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nbb|reference]
+
+With N > 1 (launched by torch.distributed.run) every rank steps an
+independent replica on its own GPU ("replicas only": the path has no
+exchange step); the elapsed time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "amsc-nbody_b200"))
+
+METRIC = "steps/s at N=2^20 θ=0.5: mixed vs FP64 path, same B200, rms force err ≤1e-3"
+N_DEFAULT = 1 << 20
+THETA, EPS, DT, G = 0.5, 0.01, 1e-3, 1.0
+L2_FLUSH_BYTES = 256 << 20
+ERROR_TARGETS = 4096
+
+
+def workload_name(n):
+    exp = int(round(math.log2(n))) if n > 0 else 0
+    size = f"2^{exp}" if (1 << exp) == n else str(n)
+    return f"plummer N={size} theta={THETA} eps={EPS} dt={DT} G={G} (seed 0)"
+
+
+# ------------------------------------------------------------ clocks ---
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------- distributed ---
+
+def dist_setup():
+    """Rank bookkeeping for torchrun launches; returns (rank, world, local)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    """Max of a per-rank scalar over all ranks (identity on one rank)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: float, world: int) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def dist_teardown(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+# --------------------------------------------------------- measuring ---
+
+def nominal_fp32_tflops(sm_mhz: float, sms: int = 148) -> float:
+    """FP32 SIMT FMA peak: SMs x 128 lanes x 2 flops x clock."""
+    return sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+
+
+def time_steps(nbb, sim, torch, stream, flush, steps):
+    """Per-step CUDA-event times (ms) of `steps` graph-replayed steps; L2 is
+    flushed between steps, outside the timed events."""
+    times = []
+    launches0 = nbb.kernel_launch_count()
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        sim.step()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return times, nbb.kernel_launch_count() - launches0
+
+
+def force_error(nbb, p, precision, targets):
+    exact = np.stack(nbb.compute_direct_accelerations(p.mass, p.x, p.y, p.z, G, EPS, targets=targets))
+    ax, ay, az = nbb.compute_accelerations(p, THETA, EPS, G, precision=precision)
+    a = np.stack([ax, ay, az])[:, targets]
+    rel = np.linalg.norm(a - exact, axis=0) / np.linalg.norm(exact, axis=0)
+    return {"rms_rel": float(np.sqrt(np.mean(rel ** 2))), "max_rel": float(rel.max()),
+            "rel_l2": float(np.linalg.norm(a - exact) / np.linalg.norm(exact)),
+            "targets": int(targets.size), "reference": "FP64 direct summation (GPU kernel)"}
+
+
+def cpu_baseline(p, budget_s=30.0):
+    """The oracle (CPU restatement of the reference pipeline) on this host:
+    one full rebuild + force evaluation over all targets (what a step costs,
+    KD/K are negligible), every core via OpenMP."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    pyoracle.pipeline(p.mass, p.x, p.y, p.z, theta=THETA, soft=EPS, g=G, n_threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "steps/s", "cores": cores, "kind": "port",
+            "sample": f"one full rebuild + force evaluation of all {len(p)} targets "
+                      f"({dt:.2f} s, OpenMP over targets)"}
+
+
+def run_nbb(args, rank, world, local):
+    import torch
+
+    import nbb
+    from nbb import ics
+
+    torch.cuda.set_device(local)
+    n = args.n
+    p = ics.plummer(n, seed=0)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    results = {}
+    sampler = ClockSampler(local)
+    sims = {}
+    for name, prec in (("mixed", nbb.PRECISION_MIXED), ("fp64", nbb.PRECISION_FP64)):
+        sim = nbb.Simulation(p, nbb.SimulationConfig(DT, THETA, EPS, G, precision=prec, device=local))
+        sim.set_stream(stream.cuda_stream)
+        sim.initialize()
+        sims[name] = sim
+    for name, sim in sims.items():
+        for _ in range(args.warmup):
+            sim.step()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        with (sampler if name == "mixed" else _Null()):
+            times, launches = time_steps(nbb, sim, torch, stream, flush, args.steps)
+        torch.cuda.synchronize()
+        barrier(world)
+        total_ms = max_over_ranks(sum(times), world)
+        stage_ms, st = sim.profile()
+        results[name] = {"ms_per_step": total_ms / args.steps, "step_ms": times, "launches": launches,
+                         "stages_ms": stage_ms, "interactions": st.interactions,
+                         "mac_tests": st.mac_tests, "n_groups": st.n_groups,
+                         "n_octree_nodes": st.n_octree_nodes}
+    # end to end through the public API: pinned host state in, step, state out
+    sim = sims["mixed"]
+    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in p.arrays()]
+    hst = [t.numpy() for t in pin]
+    sim.upload(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6])
+    torch.cuda.synchronize()
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            e0.record(stream)
+        sim.upload(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6])
+        sim.step()
+        sim.download(out=hst[1:])
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(sum(e2e_times), world) / args.steps
+    return p, results, e2e_ms, sampler.summary()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["nbb", "reference"], default="nbb")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, rank, world, local)
+        else:
+            line = bench_nbb(args, rank, world, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist_teardown(world)
+
+
+def bench_nbb(args, rank, world, local):
+    import nbb
+
+    p, res, e2e_ms, clocks = run_nbb(args, rank, world, local)
+    mixed, plain = res["mixed"], res["fp64"]
+    steps_s = world * 1000.0 / mixed["ms_per_step"]
+    plain_s = world * 1000.0 / plain["ms_per_step"]
+    line = {
+        "metric": METRIC, "value": steps_s, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 interactions / f64 state",
+        "data": "synthetic (seeded Plummer sphere)",
+        "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA, "softening": EPS,
+                   "dt": DT, "G": G, "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed between timed steps (256 MiB write, outside the step events)",
+                   "step": "CUDA-graph replay of KD + rebuild + traversal + K"},
+        "plain_fp64": {"value": plain_s, "unit": "steps/s", "ms_per_step": plain["ms_per_step"],
+                       "dtype": "f64", "stages_ms": plain["stages_ms"],
+                       "interactions": plain["interactions"]},
+        "speedup_mixed_vs_fp64": plain["ms_per_step"] / mixed["ms_per_step"],
+        "stages_ms": mixed["stages_ms"],
+        "interactions": mixed["interactions"], "mac_tests": mixed["mac_tests"],
+        "octree": {"groups": mixed["n_groups"], "nodes": mixed["n_octree_nodes"]},
+        "gpu_launches": int(mixed["launches"]),
+        "clocks": clocks,
+    }
+    # e2e: the same metric through the public API with host buffers
+    bi = 7 * args.n * 8
+    bo = 6 * args.n * 8
+    line["e2e"] = {"value": world * 1000.0 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": bi,
+                   "d2h_bytes_per_step": bo}
+    # roofline of the dominant kernel (mixed traversal): 20 flops/interaction
+    trav_ms = mixed["stages_ms"]["traversal"]
+    achieved = 20.0 * mixed["interactions"] / (trav_ms * 1e-3) / 1e12
+    peak32 = nbb.measure_fma_tflops(nbb.PRECISION_MIXED)
+    peak64 = nbb.measure_fma_tflops(nbb.PRECISION_FP64)
+    sm_mhz = clocks.get("sm_max_mhz") or 1965.0
+    line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+                        "frac": achieved / peak32, "traffic": None,
+                        "kernel": "traverse_mixed_kernel",
+                        "peak_source": "measured in this run: SIMT FP32 FMA throughput kernel "
+                                       "(MEASURED_PEAKS.json has HBM and bf16-tensor figures only; "
+                                       f"nominal {nominal_fp32_tflops(sm_mhz):.1f})",
+                        "flops_per_interaction": 20,
+                        "interactions_per_s": mixed["interactions"] / (trav_ms * 1e-3)}
+    ptrav = plain["stages_ms"]["traversal"]
+    p_ach = 20.0 * plain["interactions"] / (ptrav * 1e-3) / 1e12
+    line["plain_fp64"]["roofline"] = {"bound": "fp64", "achieved": p_ach, "peak": peak64,
+                                      "unit": "TFLOP/s", "frac": p_ach / peak64,
+                                      "kernel": "traverse_fp64_kernel",
+                                      "interactions_per_s": plain["interactions"] / (ptrav * 1e-3)}
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs")
+    if hbm:
+        # build stages are HBM-bound: bytes per particle per step
+        line["roofline"]["hbm_gbs_measured_peak"] = hbm
+    if rank == 0 and not args.no_error:
+        rng = np.random.Generator(np.random.Philox(12345))
+        tg = np.sort(rng.choice(args.n, min(ERROR_TARGETS, args.n), replace=False)).astype(np.int32)
+        line["force_error"] = {"mixed": force_error(nbb, p, nbb.PRECISION_MIXED, tg),
+                               "fp64": force_error(nbb, p, nbb.PRECISION_FP64, tg)}
+        line["valid_rms_le_1e-3"] = line["force_error"]["mixed"]["rms_rel"] <= 1e-3
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p)
+    return line if rank == 0 else None
+
+
+def run_reference(args, rank, world, local):
+    """The reference's own implementation of the step: its CUDA sources,
+    unmodified, built into oracle/_ref/libnbody_ref.so and driven through its
+    function-level API in Simulation::step order (G=1), on this GPU.  Rank 0
+    alone runs it."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+
+    from nbb import ics
+
+    p = ics.plummer(args.n, seed=0)
+    if not pyoracle.ref_available():
+        # no reference build travelled with the snapshot: time the oracle
+        # port on the host cores instead
+        base = cpu_baseline(p)
+        return {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": "steps/s",
+                "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1000.0 / base["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Plummer sphere)",
+                "config": {"workload": workload_name(args.n), "n": args.n},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    steps = args.steps
+    ms = np.zeros(args.warmup + steps, np.float32)
+    with ClockSampler(local) as sampler:
+        pyoracle.ref_simulate(p, args.warmup + steps, DT, THETA, EPS, G, step_ms=ms)
+    timed = ms[args.warmup:]
+    ms_per_step = float(timed.mean())
+    value = 1000.0 / ms_per_step
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": 1,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Plummer sphere)",
+            "config": {"workload": workload_name(args.n), "n": args.n, "theta": THETA,
+                       "softening": EPS, "dt": DT, "G": G,
+                       "implementation": "reference CUDA sources (unmodified) built for sm_100a, "
+                                         "Simulation::step order, per-step allocation and host "
+                                         "syncs as in the reference"},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 0, "kind": "reference",
+                             "sample": f"{steps} reference steps on the GPU (the reference has no "
+                                       "CPU implementation of the path)"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "clocks": sampler.summary()}
+
+
+if __name__ == "__main__":
+    main()

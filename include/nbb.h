@@ -1,0 +1,241 @@
+/*
+ * nbb.h -- C ABI of the B200-native Barnes-Hut step (libnbb.so).
+ *
+ * The entry points replace the public interface of sytrams/AMSC-Nbody's
+ * hot path; each cites the reference interface it stands in for (paths
+ * relative to that project's root).  Plain C types only: sizes, status codes
+ * and raw host or device pointers.  A header-only C++ layer with the
+ * reference's own class and function names sits on top of this ABI
+ * (amsc-nbody_b200/cpp/nbb_simulation.hpp).
+ *
+ * Status convention: every function returns an nbb_status; on failure
+ * nbb_last_error_message() describes the error in the words the reference
+ * would have thrown with, and nbb_last_error_code() carries the stage/device
+ * code.  A simulation handle that reported an error other than
+ * NBB_ERR_INVALID_ARGUMENT / NBB_ERR_LOGIC on a step is unusable afterwards,
+ * as the reference's Simulation enters State::failed
+ * (src/simulation.cpp:316-335).
+ *
+ * Threading: a handle is not thread-safe; distinct handles are independent.
+ */
+#ifndef NBB_H
+#define NBB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBB_API_VERSION 1
+
+typedef enum {
+  NBB_OK = 0,
+  NBB_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument */
+  NBB_ERR_DOMAIN = 2,           /* reference: std::domain_error (non-finite) */
+  NBB_ERR_LOGIC = 3,            /* reference: std::logic_error (call order) */
+  NBB_ERR_CUDA = 4,             /* CUDA runtime failure (runtime_error) */
+  NBB_ERR_DEVICE = 5,           /* device stage error code (runtime_error) */
+  NBB_ERR_TIMEOUT = 6,          /* a bounded device-side wait gave up */
+  NBB_ERR_OVERFLOW = 7,         /* reference: std::overflow_error */
+  NBB_ERR_NO_DEVICE = 8         /* no CUDA device / kernel image */
+} nbb_status;
+
+/* Traversal arithmetic.  FP64 is the reference's plain form
+ * (gpu/cuda_kernels/barnes_hut.cu:184-342): per-target acceptance test and
+ * interaction sets, FP64 throughout.  MIXED evaluates the interaction bulk in
+ * FP32 (offsets formed in FP64 and rounded, rsqrtf + one Newton step,
+ * Kahan-compensated partial sums) over interaction lists shared by a warp
+ * group of Morton-consecutive targets whose acceptance test is the
+ * reference's d > s/theta + delta measured from the group's bounding box. */
+typedef enum { NBB_PRECISION_FP64 = 0, NBB_PRECISION_MIXED = 1 } nbb_precision;
+
+/* SimulationConfig{timeStep, theta, softening} (src/simulation.hpp:18-22)
+ * plus BarnesHutParameters::gravitationalConstant (src/barnes_hut.hpp:8-13),
+ * which the reference's Simulation fixes to the SI value. */
+typedef struct {
+  double time_step;
+  double theta;
+  double softening;
+  double gravitational_constant;
+  int precision;  /* nbb_precision */
+  int group_size; /* MIXED: targets per warp group, 16/32/64; 0 = tuned */
+  int use_graph;  /* capture each step into a CUDA graph (default 1) */
+  int device;     /* CUDA device ordinal (default 0) */
+} nbb_config;
+
+/* Defaults of BarnesHutParameters (theta 0.5, softening 1e-6, G = SI);
+ * time_step 0 must be set by the caller. */
+void nbb_config_default(nbb_config *cfg);
+
+typedef struct nbb_sim nbb_sim;
+
+/* Simulation(Particles, SimulationConfig) (src/simulation.cpp:286-290):
+ * validates the configuration and copies the planar state in (host pointers
+ * when on_device == 0, device pointers otherwise).  type may be NULL. */
+int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass,
+                   const double *x, const double *y, const double *z,
+                   const double *vx, const double *vy, const double *vz,
+                   const uint8_t *type, int on_device, nbb_sim **out);
+
+/* Simulation::initialize (src/simulation.cpp:294-314): first spatial build
+ * and acceleration; NBB_ERR_LOGIC when called twice. */
+int nbb_sim_initialize(nbb_sim *sim);
+
+/* Simulation::step / run (src/simulation.cpp:316-343): KD, rebuild, force,
+ * K.  No host synchronisation inside a step; the call synchronises once at
+ * its end to report device errors. */
+int nbb_sim_step(nbb_sim *sim);
+int nbb_sim_run(nbb_sim *sim, uint64_t steps);
+
+/* Simulation::time / stepNumber (src/simulation.cpp:345-347) */
+double nbb_sim_time(const nbb_sim *sim);
+uint64_t nbb_sim_step_number(const nbb_sim *sim);
+
+/* Simulation::particles() -> DeviceParticlesView (src/particle.hpp:85-96):
+ * non-owning device pointers, valid until nbb_sim_destroy.  ax/ay/az hold
+ * the acceleration of the current state. */
+typedef struct {
+  size_t count;
+  double *mass, *x, *y, *z, *vx, *vy, *vz;
+  uint8_t *type;
+  double *ax, *ay, *az;
+} nbb_state_view;
+int nbb_sim_state(nbb_sim *sim, nbb_state_view *view);
+
+/* Host <-> device state transfer (positions and velocities; mass too on
+ * upload when mass != NULL).  Pinned host memory gives asynchronous copies
+ * on the simulation stream; the call returns after the copy is enqueued
+ * (upload) or complete (download). */
+int nbb_sim_upload(nbb_sim *sim, const double *mass, const double *x,
+                   const double *y, const double *z, const double *vx,
+                   const double *vy, const double *vz);
+int nbb_sim_download(nbb_sim *sim, double *x, double *y, double *z,
+                     double *vx, double *vy, double *vz);
+/* Accelerations of the current state to host memory. */
+int nbb_sim_download_accel(nbb_sim *sim, double *ax, double *ay, double *az);
+
+/* Stream control: all work of the handle goes to this stream (a
+ * cudaStream_t; NULL = the handle's own stream). */
+int nbb_sim_set_stream(nbb_sim *sim, void *stream);
+int nbb_sim_synchronize(nbb_sim *sim);
+int nbb_sim_destroy(nbb_sim *sim);
+
+/* Counters of the last force evaluation. */
+typedef struct {
+  int n_groups;         /* unique Morton keys G */
+  int n_octree_nodes;   /* M */
+  int64_t interactions; /* monopole + leaf-pair interactions evaluated */
+  int64_t mac_tests;    /* acceptance tests evaluated */
+} nbb_stats;
+int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats);
+
+/* Diagnostic: recompute the force of the current state (no kick, no drift,
+ * state unchanged) outside the step graph, with CUDA events between the
+ * stages.  stage_ms receives NBB_PROFILE_STAGES durations in milliseconds:
+ * reset, bounding box, Morton + sort + groups, tree build, traversal. */
+#define NBB_PROFILE_STAGES 5
+int nbb_sim_profile(nbb_sim *sim, float *stage_ms, nbb_stats *stats);
+
+/* Every intermediate of the last spatial build, for bit-exact comparison
+ * with the reference's MortonKeys / MortonLeafGroups / Tree /
+ * RadixToOctreePlan / Octree structures.  The caller provides host buffers
+ * (any may be NULL) with capacities: n for keys/idx/groups, n-1 for radix
+ * internal arrays, 2n-1 for radix-node arrays, m_capacity octree nodes
+ * (children 8*m_capacity).  Sizes are returned in n_groups / n_octree. */
+typedef struct {
+  double box[4];                                  /* Bbox centre + side */
+  uint32_t *keys, *idx;                           /* MortonKeys */
+  uint32_t *uniq;                                 /* MortonLeafGroups */
+  int *gfirst, *gcount;
+  int *left, *right, *rfirst, *rlast, *plen;      /* Tree (G-1) */
+  int *rparent;                                   /* Tree (2G-1) */
+  int *plan_level, *plan_count, *plan_offset;     /* RadixToOctreePlan */
+  int m_capacity;
+  int *children, *oparent, *olevel;               /* Octree topology */
+  uint32_t *oprefix;
+  int *ofirst, *ocount, *child_count;
+  double *cx, *cy, *cz, *half;                    /* Octree geometry */
+  double *mass, *comx, *comy, *comz;              /* Octree physics */
+  int n_groups, n_octree;
+} nbb_tree_export;
+int nbb_sim_export(nbb_sim *sim, nbb_tree_export *out);
+
+/* ---------------------------------------------------- function level ---- */
+
+/* One spatial build + Barnes-Hut evaluation on caller particles, the
+ * sequence Bbox -> MortonKeys -> allocate/build{MortonLeafGroups, Tree,
+ * RadixToOctreePlan, Octree, geometry, physics} ->
+ * computeBarnesHutAcceleration (src/simulation.cpp:353-414,
+ * gpu/cuda_kernels/barnes_hut.cu:345-391).  Accelerations are written at the
+ * original particle index.  Pointers are host (on_device == 0) or device.
+ * export_out and stats may be NULL. */
+int nbb_accel(size_t n, const double *mass, const double *x, const double *y,
+              const double *z, double theta, double softening, double g,
+              int precision, double *ax, double *ay, double *az,
+              int on_device, nbb_tree_export *export_out, nbb_stats *stats);
+
+/* FP64 direct summation (the theta-error oracle of
+ * tests/integration/cuda/barnes_hut_accuracy_test.cu:101-172) for the
+ * n_targets particle indices in targets (NULL: all n).  Output k belongs to
+ * targets[k]. */
+int nbb_accel_direct(size_t n, const double *mass, const double *x,
+                     const double *y, const double *z, int n_targets,
+                     const int *targets, double g, double softening,
+                     double *ax, double *ay, double *az, int on_device);
+
+/* computeBarnesHutAcceleration on a caller-built octree
+ * (gpu/cuda_kernels/barnes_hut.cu:345-391), FP64 plain form.  Octree arrays
+ * follow src/octree_types.hpp:73-104 (children node-major, 8 per node; root
+ * 0).  particle_order: 0 = original, 1 = morton (BarnesHutParticleOrder). */
+typedef struct {
+  int n_nodes, n_particles;
+  const int *children, *parent, *first, *count;
+  const double *mass, *comx, *comy, *comz;
+  const double *cx, *cy, *cz, *half;
+} nbb_octree_view;
+int nbb_accel_octree(const nbb_octree_view *octree, const uint32_t *idx,
+                     const double *mass, const double *x, const double *y,
+                     const double *z, double *ax, double *ay, double *az,
+                     double theta, double softening, double g,
+                     int particle_order, int on_device);
+
+/* leapfrogKickDrift / leapfrogKick (src/integrator.hpp:5-7).  Pointers are
+ * device pointers, as in the reference; dt must be finite and positive. */
+int nbb_kick_drift(double *x, double *y, double *z, double *vx, double *vy,
+                   double *vz, const double *ax, const double *ay,
+                   const double *az, size_t n, double dt, void *stream);
+int nbb_kick(double *vx, double *vy, double *vz, const double *ax,
+             const double *ay, const double *az, size_t n, double dt,
+             void *stream);
+
+/* buildMortonLeafGroups -> buildTreeFromMortonGroups ->
+ * buildRadixToOctreePlan -> buildSparseOctreeTopology on caller sorted keys
+ * (src/morton_leaf_groups.hpp:43-47, src/tree_builder.hpp:5-13,
+ * src/radix_to_octree.hpp:67-70, src/octree_builder.hpp:7-11).  Host
+ * pointers; outputs into out (geometry/physics fields are left untouched). */
+int nbb_octree_from_keys(const uint32_t *sorted_keys, int n,
+                         nbb_tree_export *out);
+
+/* buildTree on caller keys (src/tree_builder.hpp:9), any 32-bit keys,
+ * duplicates allowed.  Host pointers; left..plen n-1 entries, parent 2n-1. */
+int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right,
+                   int *rfirst, int *rlast, int *plen, int *parent);
+
+/* Diagnostic: measured SIMT FMA throughput of the current device in TFLOP/s
+ * (precision NBB_PRECISION_FP64 or NBB_PRECISION_MIXED = FP32), the
+ * roofline denominator of the traversal kernels. */
+int nbb_measure_fma_tflops(int precision, double *tflops);
+
+/* Last error of the calling thread. */
+const char *nbb_last_error_message(void);
+int nbb_last_error_code(void);
+
+/* Number of kernels this library launched in the calling process. */
+uint64_t nbb_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
