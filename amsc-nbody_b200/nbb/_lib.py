@@ -83,7 +83,7 @@ SIGNATURES = {
     "nbb_sim_export": (_I, [_P, _P]),
     "nbb_accel": (_I, [_Z, _P, _P, _P, _P, _D, _D, _D, _I, _P, _P, _P, _I, _P, _P]),
     "nbb_accel_direct": (_I, [_Z, _P, _P, _P, _P, _I, _P, _D, _D, _P, _P, _P, _I]),
-    "nbb_accel_octree": (_I, [_P] * 10 + [_D, _D, _D, _I, _I]),
+    "nbb_accel_octree": (_I, [_P] * 9 + [_D, _D, _D, _I, _I]),
     "nbb_kick_drift": (_I, [_P] * 9 + [_Z, _D, _P]),
     "nbb_kick": (_I, [_P] * 6 + [_Z, _D, _P]),
     "nbb_octree_from_keys": (_I, [_P, _I, _P]),
