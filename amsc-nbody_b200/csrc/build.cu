@@ -23,6 +23,7 @@
 #include "nbb_internal.cuh"
 
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 namespace nbb {
@@ -50,6 +51,7 @@ __global__ void reset_scalars_kernel(DevScalars *sc) {
     sc->ticket_encode = 0;
     for (int k = 0; k < 8; ++k) sc->tile_counter[k] = 0;
     sc->work_counter = 0;
+    sc->n_tgroups = 0;
     sc->stack_overflow = 0;
     sc->interactions = 0;
     sc->mac_tests = 0;
@@ -668,6 +670,8 @@ __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
     ws.child_count[i] = 0;
     ws.subtree[i] = 0;
     ws.preoff[i] = 0;
+    ws.psub[i] = 0;
+    ws.pfirst[i] = INT_MAX;
     ws.mass[i] = 0.0;
     ws.comx[i] = 0.0;
     ws.comy[i] = 0.0;
@@ -876,6 +880,8 @@ __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
       ws.comz[node] = __dmul_rn(wz, inv);
     }
     ws.subtree[node] = 1;
+    ws.psub[node] = pc;
+    ws.pfirst[node] = f;
   }
 }
 
@@ -920,6 +926,8 @@ __global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
       const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
       double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
       int size = 1;
+      int nparticles = 0;
+      int firstp = INT_MAX;
       int sub[8];
 #pragma unroll
       for (int o = 0; o < 8; ++o) {
@@ -933,6 +941,8 @@ __global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
         wz = __fma_rn(cm, __ldcg(ws.comz + c), wz);
         sub[o] = __ldcg(ws.subtree + c);
         size += sub[o];
+        nparticles += __ldcg(ws.psub + c);
+        firstp = min(firstp, __ldcg(ws.pfirst + c));
       }
       ws.mass[parent] = tm;
       if (tm > 0.0) {
@@ -953,6 +963,8 @@ __global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
         run += sub[o];
       }
       ws.subtree[parent] = size;
+      ws.psub[parent] = nparticles;
+      ws.pfirst[parent] = firstp;
       done = parent;
       parent = ws.oparent[done];
     }
@@ -1029,6 +1041,82 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
   }
 }
 
+// ------------------------------------------------------ target groups ---
+
+// Target groups for the traversal: every node holding more than kGroupMax
+// particles packs its children with at most kGroupMax particles, in octant
+// (= Morton) order, greedily into runs of at most kGroupMax particles; each
+// run is one group.  Groups are contiguous ranges of the sorted particles,
+// never larger than kGroupMax and never wider than their parent cell, so a
+// warp's targets stay spatially compact (fixed 32-particle slices of the
+// Morton order can straddle the whole system where the curve jumps).
+__global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    const int np = ws.psub[node];
+    if (np <= kGroupMax) {
+      if (node == 0 && np > 0) ws.tflag[0] = 1;  // the whole system is one group
+      continue;
+    }
+    int run = 0;
+    for (int o = 0; o < 8; ++o) {
+      const int c = ws.children[(size_t)node * 8 + o];
+      if (c <= 0 || c >= m) continue;
+      const int cp = ws.psub[c];
+      if (cp > kGroupMax) {
+        run = 0;
+        continue;
+      }
+      if (run == 0 || run + cp > kGroupMax) {
+        const int f = ws.pfirst[c];
+        if (f >= 0 && f < ws.n) ws.tflag[f] = 1;
+        run = 0;
+      }
+      run += cp;
+    }
+  }
+}
+
+// Compaction of the group-start flags into the list of group starts.
+__global__ void __launch_bounds__(kScanThreads) group_scan_kernel(Workspace ws) {
+  __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
+  __shared__ unsigned long long s_total, s_prefix;
+  __shared__ int s_tile;
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int n = ws.n;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[6], 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  const int base = tile * kScanTile;
+  if (base >= n) return;
+  int flag[kScanItems], excl[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    flag[k] = (i < n) ? (int)ws.tflag[i] : 0;
+  }
+  const unsigned long long total = block_scan_rows<kScanItems, kScanThreads>(flag, excl, row_warp, &s_total);
+  if (threadIdx.x < 32) {
+    const unsigned long long p = warp_lookback(ws.scan_status + ws.scan_tiles_n + ws.scan_tiles_r, tile,
+                                               total, sc, kStageGroups);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  const int prefix = (int)s_prefix;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    if (i < n && flag[k]) {
+      const int g = prefix + excl[k];
+      if (g >= 0 && g < n) ws.tstart[g] = i;
+    }
+  }
+  if (base + kScanTile >= n && threadIdx.x == 0) sc->n_tgroups = prefix + (int)total;
+}
+
 // Reference-layout keys only (no particles): used by the function-level
 // topology entry points.
 __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
@@ -1048,8 +1136,12 @@ cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s) {
   e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)kSortPasses * ws.sort_tiles * 256, s);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(ws.scan_status, 0,
-                      sizeof(unsigned long long) * (size_t)(ws.scan_tiles_n + ws.scan_tiles_r), s);
+                      sizeof(unsigned long long) * (size_t)(2 * ws.scan_tiles_n + ws.scan_tiles_r), s);
   if (e != cudaSuccess) return e;
+  if (ws.tflag) {
+    e = cudaMemsetAsync(ws.tflag, 0, (size_t)ws.n, s);
+    if (e != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
 
@@ -1091,7 +1183,9 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   node_init_kernel<<<grid, kBlock, 0, s>>>(ws);
   propagate_kernel<<<grid, kBlock, 0, s>>>(ws);
   layout_kernel<<<grid, kBlock, 0, s>>>(ws, theta);
-  count_launches(7);
+  group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  count_launches(9);
   return cudaGetLastError();
 }
 

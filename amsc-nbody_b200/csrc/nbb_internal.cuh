@@ -45,6 +45,7 @@ struct DevScalars {
   unsigned int ticket_encode;
   unsigned int tile_counter[8];  // dynamic tile ids of single-pass kernels
   unsigned int work_counter;     // traversal work queue
+  int n_tgroups;                 // traversal target groups
   unsigned int stack_overflow;   // mixed traversal nodes accepted on overflow
   unsigned long long interactions;
   unsigned long long mac_tests;
@@ -55,6 +56,9 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs
 constexpr int kSortPasses = 4;                        // 8-bit digits, bits 32..63
+
+// Largest target group (one target per lane of a warp).
+constexpr int kGroupMax = 32;
 
 // Single-pass scan tiling.
 constexpr int kScanThreads = 256;
@@ -82,7 +86,7 @@ struct Workspace {
   uint32_t *digit_hist = nullptr;    // kSortPasses * 256 (counts -> offsets)
   uint32_t *sort_status = nullptr;   // kSortPasses * tiles * 256
   int sort_tiles = 0;
-  unsigned long long *scan_status = nullptr;  // 2 * scan tiles (groups, plan)
+  unsigned long long *scan_status = nullptr;  // scan tiles: groups, plan, target groups
   int scan_tiles_n = 0;   // tiles over n
   int scan_tiles_r = 0;   // tiles over 2n-1
 
@@ -109,6 +113,12 @@ struct Workspace {
   double *cx = nullptr, *cy = nullptr, *cz = nullptr, *half = nullptr;
   double *mass = nullptr, *comx = nullptr, *comy = nullptr, *comz = nullptr;
   int *subtree = nullptr, *preoff = nullptr;
+  int *psub = nullptr, *pfirst = nullptr;  // particles in a subtree / its first
+
+  // traversal target groups: contiguous Morton ranges of <= kGroupMax
+  // particles inside one parent cell
+  unsigned char *tflag = nullptr;  // n, 1 where a target group starts
+  int *tstart = nullptr;           // n, start of each target group
 
   // traversal layout: depth-first preorder, children visited octant 7 -> 0
   double4 *node_a = nullptr;  // com x, y, z, mass

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
   const int lane = threadIdx.x & 31;
   const int n = ws.n;
   const int m = sc->n_nodes;
-  const int n_groups = (n + 31) >> 5;
+  const int n_groups = sc->n_tgroups;
   const double soft2 = __dmul_rn(p.soft, p.soft);
   const double g = p.g;
   long long inter = 0, tests = 0;
@@ -72,8 +72,10 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
     if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
     grp = __shfl_sync(kFull, grp, 0);
     if (grp >= n_groups) break;
-    const int s = grp * 32 + lane;
-    const bool valid = s < n;
+    const int g0 = ws.tstart[grp];
+    const int g1 = (grp + 1 < n_groups) ? ws.tstart[grp + 1] : n;
+    const int s = g0 + lane;
+    const bool valid = s < g1 && s < n;
     double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
     if (valid) t = ws.pm4[s];
     double ax = 0.0, ay = 0.0, az = 0.0;
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
   int *src = sh.src[wid];
   const int n = ws.n;
   const int m = sc->n_nodes;
-  const int n_groups = (n + 31) >> 5;
+  const int n_groups = sc->n_tgroups;
   const float eps2 = (float)(p.soft * p.soft);
   const unsigned lt = lanemask_lt();
   long long inter = 0, tests = 0;
@@ -247,9 +249,11 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
     if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
     grp = __shfl_sync(kFull, grp, 0);
     if (grp >= n_groups) break;
-    const int s = grp * 32 + lane;
-    const bool valid = s < n;
-    const double4 t = ws.pm4[valid ? s : grp * 32];
+    const int g0 = ws.tstart[grp];
+    const int g1 = (grp + 1 < n_groups) ? ws.tstart[grp + 1] : n;
+    const int s = g0 + lane;
+    const bool valid = s < g1 && s < n;
+    const double4 t = ws.pm4[valid ? s : g0];
     double lo[3] = {t.x, t.y, t.z}, hi[3] = {t.x, t.y, t.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {

@@ -21,7 +21,10 @@ FLOAT_RTOL = 1e-12
 MIXED_RMS_BOUND = 1e-3
 
 
-def _compare(out, ref, ints=INT_FIELDS, floats=FLOAT_FIELDS, rtol=FLOAT_RTOL):
+def _compare(out, ref, ints=INT_FIELDS, floats=FLOAT_FIELDS, rtol=FLOAT_RTOL, bitwise=True):
+    """Integers bit-exact; floats within rtol (the bar), and -- because the
+    plain path performs the reference's operations in the reference's order
+    with the same roundings -- also bit-identical when `bitwise`."""
     assert out["n_groups"] == int(ref["n_groups"])
     assert out["n_octree"] == int(ref["n_octree"])
     assert np.array_equal(out["box"], np.asarray(ref["box"]))
@@ -31,6 +34,8 @@ def _compare(out, ref, ints=INT_FIELDS, floats=FLOAT_FIELDS, rtol=FLOAT_RTOL):
     for k in floats:
         worst[k] = rel_err(out[k], ref[k])
         assert worst[k] <= rtol, (k, worst[k])
+        if bitwise:
+            assert np.array_equal(out[k], np.asarray(ref[k])), (k, "not bit-identical", worst[k])
     return worst
 
 
@@ -340,10 +345,22 @@ def test_failed_step_poisons_simulation(nbb_mod):
 
 # ------------------------------------------------------ mixed form ---
 
+def _rms_rel(approx, exact):
+    rel = np.linalg.norm(approx - exact, axis=0) / np.linalg.norm(exact, axis=0)
+    return float(np.sqrt(np.mean(rel ** 2)))
+
+
 @pytest.mark.parametrize("recipe,n,theta,soft", [("plummer", 65536, 0.5, 0.01),
+                                                 ("plummer", 262144, 0.5, 0.01),
                                                  ("disk", 65536, 0.5, 0.005),
-                                                 ("blobs", 65536, 0.5, 1e-3)])
-def test_mixed_force_error_bound(nbb_mod, recipe, n, theta, soft):
+                                                 ("blobs", 65536, 0.3, 1e-3),
+                                                 ("blobs", 65536, 0.5, 1e-3),
+                                                 ("blobs", 65536, 0.7, 1e-3)])
+def test_mixed_force_error(nbb_mod, recipe, n, theta, soft):
+    """Mixed-form force error against FP64 direct summation: never worse
+    than the reference's own per-target acceptance test in FP64 (the group
+    test is stricter, FP32 rounding is far below the Barnes-Hut error), and
+    within the headline's RMS bound of 1e-3 on the Plummer sphere."""
     from nbb import ics
 
     p = {"plummer": lambda: ics.plummer(n, seed=0), "disk": lambda: ics.disk_bulge(n, seed=1),
@@ -351,16 +368,13 @@ def test_mixed_force_error_bound(nbb_mod, recipe, n, theta, soft):
     rng = np.random.Generator(np.random.Philox(99))
     tg = np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32)
     exact = np.stack(nbb_mod.compute_direct_accelerations(p.mass, p.x, p.y, p.z, 1.0, soft, targets=tg))
-    ax, ay, az = nbb_mod.compute_accelerations(p, theta, soft, 1.0, precision=nbb_mod.PRECISION_MIXED)
-    approx = np.stack([ax, ay, az])[:, tg]
-    rel = np.linalg.norm(approx - exact, axis=0) / np.linalg.norm(exact, axis=0)
-    rms = float(np.sqrt(np.mean(rel ** 2)))
-    assert rms <= MIXED_RMS_BOUND, rms
-    pa, pb, pc = nbb_mod.compute_accelerations(p, theta, soft, 1.0)
-    plain = np.stack([pa, pb, pc])[:, tg]
-    rel_p = np.linalg.norm(plain - exact, axis=0) / np.linalg.norm(exact, axis=0)
-    # the group acceptance test is stricter than the per-target one
-    assert rms <= float(np.sqrt(np.mean(rel_p ** 2))) * 1.05
+    mixed = np.stack(nbb_mod.compute_accelerations(p, theta, soft, 1.0, precision=nbb_mod.PRECISION_MIXED))
+    plain = np.stack(nbb_mod.compute_accelerations(p, theta, soft, 1.0))
+    rms_mixed = _rms_rel(mixed[:, tg], exact)
+    rms_plain = _rms_rel(plain[:, tg], exact)
+    assert rms_mixed <= rms_plain * 1.05, (rms_mixed, rms_plain)
+    if recipe == "plummer":
+        assert rms_mixed <= MIXED_RMS_BOUND, rms_mixed
 
 
 def test_mixed_theta_zero_is_direct(nbb_mod):
