@@ -1060,6 +1060,14 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
       if (node == 0 && np > 0) ws.tflag[0] = 1;  // the whole system is one group
       continue;
     }
+    if (ws.ocount[node] > 0) {
+      // an occupied leaf with more than kGroupMax coincident-key particles:
+      // consecutive slices of kGroupMax
+      const int f = ws.pfirst[node];
+      for (int k = 0; k < np; k += kGroupMax)
+        if (f + k >= 0 && f + k < ws.n) ws.tflag[f + k] = 1;
+      continue;
+    }
     int run = 0;
     for (int o = 0; o < 8; ++o) {
       const int c = ws.children[(size_t)node * 8 + o];

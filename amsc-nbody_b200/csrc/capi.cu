@@ -204,6 +204,11 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
 
 bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
 
+// The plain walk's per-lane acceptance test tolerates wide warps and prefers
+// full ones (fixed 32-particle slices); the mixed walk shares one acceptance
+// test per warp and needs compact octree target groups.
+int default_group_mode(int precision) { return precision == NBB_PRECISION_MIXED ? 1 : 0; }
+
 template <typename T>
 cudaError_t d2h_opt(T *dst, const T *src, size_t count, cudaStream_t s) {
   if (dst == nullptr || count == 0) return cudaSuccess;
@@ -405,6 +410,7 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   tp.kick = kick;
   tp.precision = sim->cfg.precision;
   tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size : 32;
+  tp.group_mode = default_group_mode(tp.precision);
   return tp;
 }
 
@@ -662,6 +668,7 @@ int nbb_accel(size_t n, const double *mass, const double *x, const double *y, co
   tp.soft = softening;
   tp.g = g;
   tp.precision = precision;
+  tp.group_mode = default_group_mode(precision);
   NBB_CUDA(enqueue_rebuild_force(ws, tp, 0.0, 0, sc.s), "Barnes-Hut evaluation");
   int st = check_device(ws, sc.s);
   if (st) return st;

@@ -188,6 +188,9 @@ struct TraversalParams {
   int kick = 0;
   int precision = 0;     // 0 FP64 plain, 1 mixed
   int group_size = 32;
+  // warp target sets: 0 = fixed slices of 32 consecutive Morton-ordered
+  // particles, 1 = octree target groups (contiguous, inside one parent cell)
+  int group_mode = 0;
 };
 
 // Launch-count bookkeeping (kernels launched by this library).

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
   const int lane = threadIdx.x & 31;
   const int n = ws.n;
   const int m = sc->n_nodes;
-  const int n_groups = sc->n_tgroups;
+  const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
   const double soft2 = __dmul_rn(p.soft, p.soft);
   const double g = p.g;
   long long inter = 0, tests = 0;
@@ -72,8 +72,8 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
     if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
     grp = __shfl_sync(kFull, grp, 0);
     if (grp >= n_groups) break;
-    const int g0 = ws.tstart[grp];
-    const int g1 = (grp + 1 < n_groups) ? ws.tstart[grp + 1] : n;
+    const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
+    const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
     const int s = g0 + lane;
     const bool valid = s < g1 && s < n;
     double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
   int *src = sh.src[wid];
   const int n = ws.n;
   const int m = sc->n_nodes;
-  const int n_groups = sc->n_tgroups;
+  const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
   const float eps2 = (float)(p.soft * p.soft);
   const unsigned lt = lanemask_lt();
   long long inter = 0, tests = 0;
@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
     if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
     grp = __shfl_sync(kFull, grp, 0);
     if (grp >= n_groups) break;
-    const int g0 = ws.tstart[grp];
-    const int g1 = (grp + 1 < n_groups) ? ws.tstart[grp + 1] : n;
+    const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
+    const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
     const int s = g0 + lane;
     const bool valid = s < g1 && s < n;
     const double4 t = ws.pm4[valid ? s : g0];
