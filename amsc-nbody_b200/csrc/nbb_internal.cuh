@@ -72,6 +72,7 @@ struct Workspace {
   int num_sms = 0;
   int fp64_grid = 0;    // persistent traversal grids (blocks)
   int mixed_grid = 0;
+  int mixed_grid_src = 0;
 
   // particle state, original order (SoA, FP64)
   double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;

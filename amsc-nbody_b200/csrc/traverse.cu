@@ -154,21 +154,35 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
 
 // ------------------------------------------------------------ mixed ----
 
-constexpr int kMixedWarps = 4;
-constexpr int kStackCap = 1536;
-constexpr int kListCap = 64;
+// Compile-time tuning of the mixed walk (warps per block, minimum resident
+// blocks per SM for the register budget).
+#ifndef NBB_MIXED_WARPS
+#define NBB_MIXED_WARPS 2
+#endif
+#ifndef NBB_MIXED_MINBLOCKS
+#define NBB_MIXED_MINBLOCKS 12
+#endif
+constexpr int kMixedWarps = NBB_MIXED_WARPS;
+constexpr int kStackCap = 512;
+constexpr int kListCap = 96;
 
+template <bool kTrackSource>
 struct MixedShared {
   int stack[kMixedWarps][kStackCap];
   float4 list[kMixedWarps][kListCap];
-  int src[kMixedWarps][kListCap];
+  int src[kMixedWarps][kTrackSource ? kListCap : 1];
 };
 
 // Evaluate `count` list entries for this lane's target: FP32 offsets, rsqrtf
 // plus one Newton step, plain FP32 partial sum over the batch, then one
 // Kahan-compensated addition of the batch partial into the running sum.
-// Returns true when a non-self entry coincides with the target at zero
-// softening (the reference's singular-interaction error).
+//
+// With positive softening the target's own entry (a leaf particle equal to
+// the target) has offset exactly (0, 0, 0) -- both offsets are rounded from
+// the same FP64 difference -- and contributes exactly zero, so no source
+// index is needed.  With zero softening the source index excludes self and
+// detects the reference's singular interaction (returns true).
+template <bool kTrackSource>
 __device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, int count, int self,
                                            float tx, float ty, float tz, float eps2, float3 &sum,
                                            float3 &comp) {
@@ -177,15 +191,16 @@ __device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, i
 #pragma unroll 8
   for (int j = 0; j < count; ++j) {
     const float4 e = list[j];
-    const int sidx = src[j];
     const float dx = e.x - tx, dy = e.y - ty, dz = e.z - tz;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
     float r = rsqrtf(r2);
     r = r * fmaf(-0.5f * r2, r * r, 1.5f);
-    const bool other = sidx != self;
-    const bool use = other && (r2 > 0.f);
-    singular |= other && !(r2 > 0.f) && e.w != 0.f;
-    const float f = use ? e.w * (r * r * r) : 0.f;
+    float f = e.w * (r * r * r);
+    if (kTrackSource) {
+      const bool other = src[j] != self;
+      singular |= other && !(r2 > 0.f) && e.w != 0.f;
+      f = (other && r2 > 0.f) ? f : 0.f;
+    }
     px = fmaf(f, dx, px);
     py = fmaf(f, dy, py);
     pz = fmaf(f, dz, pz);
@@ -197,38 +212,50 @@ __device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, i
   return singular;
 }
 
-// Evaluate the first 32 list entries and shift the remainder down.
-__device__ __forceinline__ void flush32(float4 *list, int *src, int &ls, int self, bool valid,
-                                        float tx, float ty, float tz, float eps2, float3 &sum,
-                                        float3 &comp, long long &inter, bool &singular) {
+// Evaluate full batches of 32 from the front of the list, shifting the
+// remainder down, until fewer than 32 entries are left.
+template <bool kTrackSource>
+__device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, int self, bool valid,
+                                           float tx, float ty, float tz, float eps2, float3 &sum,
+                                           float3 &comp, long long &inter, bool &singular) {
   const int lane = threadIdx.x & 31;
-  const bool sg = eval_batch(list, src, 32, self, tx, ty, tz, eps2, sum, comp);
-  if (valid) {
-    inter += 32;
-    singular |= sg;
+  int done = 0;
+  while (ls - done >= 32) {
+    const bool sg = eval_batch<kTrackSource>(list + done, src + (kTrackSource ? done : 0), 32, self,
+                                             tx, ty, tz, eps2, sum, comp);
+    if (valid) {
+      inter += 32;
+      singular |= sg;
+    }
+    done += 32;
   }
-  __syncwarp();
-  if (lane < ls - 32) {
-    list[lane] = list[32 + lane];
-    src[lane] = src[32 + lane];
+  if (done) {
+    __syncwarp();
+    const int rest = ls - done;
+    if (lane < rest) {
+      list[lane] = list[done + lane];
+      if (kTrackSource) src[lane] = src[done + lane];
+    }
+    ls = rest;
+    __syncwarp();
   }
-  ls -= 32;
-  __syncwarp();
 }
 
-// Mixed-precision traversal, one warp per group of 32 Morton-consecutive
-// targets.  The group's bounding box (FP64) replaces the target in the
-// reference's acceptance test: a node is accepted for the whole group when
-// the box does not touch the cell and the box-to-centre-of-mass distance
-// exceeds crit = side/theta + |com - centre|, which implies acceptance for
-// every target in the box.  Nodes are examined 32 at a time (one per lane)
-// from a warp-private stack in shared memory; accepted nodes and the
-// particles of reached leaves go to a shared interaction list as FP32
-// offsets from the group centre (formed in FP64, then rounded) and are
-// evaluated by all 32 lanes in batches of 32.
-__global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Workspace ws,
+// Mixed-precision traversal, one warp per target group (at most 32
+// Morton-consecutive targets inside one parent cell).  The group's bounding
+// box (FP64) replaces the target in the reference's acceptance test: a node
+// is accepted for the whole group when the box does not touch the cell and
+// the box-to-centre-of-mass distance exceeds crit = side/theta +
+// |com - centre|, which implies acceptance for every target in the box.
+// Nodes are examined 32 at a time (one per lane) from a warp-private stack
+// in shared memory, each lane fetching its node's record and child list in
+// one round trip; accepted nodes and the particles of reached leaves go to a
+// shared interaction list as FP32 offsets from the group centre (formed in
+// FP64, then rounded) and are evaluated by all lanes in batches of 32.
+template <bool kTrackSource>
+__global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) traverse_mixed_kernel(Workspace ws,
                                                                           TraversalParams p) {
-  __shared__ MixedShared sh;
+  __shared__ MixedShared<kTrackSource> sh;
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int lane = threadIdx.x & 31;
@@ -278,29 +305,32 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
       sp -= k;
       __syncwarp();
       int cat = 0;  // 0 nothing, 1 accepted cell, 2 leaf, 3 open
-      int4 meta = make_int4(0, 0, 0, 0);
-      double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+      int4 meta = make_int4(0, 0, 0, 0), kid0 = make_int4(-1, -1, -1, -1), kid1 = kid0;
+      double4 a = make_double4(0.0, 0.0, 0.0, 0.0), b = a;
+      double crit = 0.0;
       if (node >= 0) {
+        // one round trip: record, geometry, radius and children together
         meta = ws.node_meta[node];
+        a = ws.node_a[node];
+        b = ws.node_b[node];
+        crit = ws.node_c[node].x;
+        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)node * 8);
+        kid0 = kids[0];
+        kid1 = kids[1];
         if (meta.z > 0) {
           cat = 2;
-        } else {
-          a = ws.node_a[node];
-          if (a.w != 0.0) {
-            const double4 b = ws.node_b[node];
-            const double crit = ws.node_c[node].x;
-            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
-            bool overlap = true;
-            double d2 = 0.0;
+        } else if (a.w != 0.0) {
+          const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
+          bool overlap = true;
+          double d2 = 0.0;
 #pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-              overlap = overlap && hi[ax] >= cen[ax] - b.w && lo[ax] <= cen[ax] + b.w;
-              const double e = fmax(0.0, fmax(lo[ax] - com[ax], com[ax] - hi[ax]));
-              d2 = fma(e, e, d2);
-            }
-            ++tests;
-            cat = (!overlap && sqrt(d2) > crit) ? 1 : 3;
+          for (int ax = 0; ax < 3; ++ax) {
+            overlap = overlap && hi[ax] >= cen[ax] - b.w && lo[ax] <= cen[ax] + b.w;
+            const double e = fmax(0.0, fmax(lo[ax] - com[ax], com[ax] - hi[ax]));
+            d2 = fma(e, e, d2);
           }
+          ++tests;
+          cat = (!overlap && d2 > crit * crit) ? 1 : 3;
         }
       }
       // opened nodes push their children; a push that would not fit the
@@ -322,11 +352,10 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
       if (nch > 0) {
         // children always follow their parent in preorder; anything else is
         // dropped so the walk stays finite
-        const int *kids = ws.node_kids + (size_t)node * 8;
-        for (int j = 0; j < nch; ++j) {
-          const int c = kids[j];
-          stack[sp + excl + j] = (c > node && c < m) ? c : -1;
-        }
+        const int kid[8] = {kid0.x, kid0.y, kid0.z, kid0.w, kid1.x, kid1.y, kid1.z, kid1.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j < nch) stack[sp + excl + j] = (kid[j] > node && kid[j] < m) ? kid[j] : -1;
       }
       sp += pushed;
       // accepted cells -> interaction list
@@ -334,33 +363,52 @@ __global__ void __launch_bounds__(kMixedWarps * 32) traverse_mixed_kernel(Worksp
       if (cat == 1) {
         const int pos = ls + __popc(cm & lt);
         list[pos] = make_float4((float)(a.x - gcx), (float)(a.y - gcy), (float)(a.z - gcz), (float)a.w);
-        src[pos] = -1;
+        if (kTrackSource) src[pos] = -1;
       }
       ls += __popc(cm);
-      __syncwarp();
-      while (ls >= 32) flush32(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
-      // reached leaves -> their particles, 32 at a time
-      unsigned lm = __ballot_sync(kFull, cat == 2);
-      while (lm) {
-        const int l = __ffs(lm) - 1;
-        lm &= lm - 1;
-        const int first = __shfl_sync(kFull, meta.y, l);
-        const int cnt = __shfl_sync(kFull, meta.z, l);
-        for (int b0 = 0; b0 < cnt; b0 += 32) {
-          const int j = b0 + lane;
-          if (j < cnt) {
-            const double4 q = ws.pm4[first + j];
-            list[ls + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
-            src[ls + lane] = first + j;
+      // reached leaves -> their particles: all at once when they fit
+      const int lc = (cat == 2) ? meta.z : 0;
+      int linc = lc;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kFull, linc, o);
+        if (lane >= o) linc += v;
+      }
+      const int ltotal = __shfl_sync(kFull, linc, 31);
+      if (ls + ltotal <= kListCap) {
+        for (int j = 0; j < lc; ++j) {
+          const double4 q = ws.pm4[meta.y + j];
+          const int pos = ls + linc - lc + j;
+          list[pos] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+          if (kTrackSource) src[pos] = meta.y + j;
+        }
+        ls += ltotal;
+        __syncwarp();
+        flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+      } else {
+        __syncwarp();
+        flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+        unsigned lm = __ballot_sync(kFull, cat == 2);
+        while (lm) {
+          const int l = __ffs(lm) - 1;
+          lm &= lm - 1;
+          const int first = __shfl_sync(kFull, meta.y, l);
+          const int cnt = __shfl_sync(kFull, meta.z, l);
+          for (int b0 = 0; b0 < cnt; b0 += 32) {
+            const int j = b0 + lane;
+            if (j < cnt) {
+              const double4 q = ws.pm4[first + j];
+              list[ls + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+              if (kTrackSource) src[ls + lane] = first + j;
+            }
+            ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
+            __syncwarp();
+            flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
           }
-          ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
-          __syncwarp();
-          if (ls >= 32) flush32(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
         }
       }
     }
     if (ls > 0) {
-      const bool sg = eval_batch(list, src, ls, s, tx, ty, tz, eps2, sum, comp);
+      const bool sg = eval_batch<kTrackSource>(list, src, ls, s, tx, ty, tz, eps2, sum, comp);
       if (valid) {
         inter += ls;
         singular |= sg;
@@ -657,17 +705,22 @@ cudaError_t configure_traversal(Workspace &ws) {
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_fp64_kernel, 256, 0);
   if (e != cudaSuccess) return e;
   ws.fp64_grid = sms * (per_sm > 0 ? per_sm : 1);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel, kMixedWarps * 32, 0);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel<false>, kMixedWarps * 32, 0);
   if (e != cudaSuccess) return e;
   ws.mixed_grid = sms * (per_sm > 0 ? per_sm : 1);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel<true>, kMixedWarps * 32, 0);
+  if (e != cudaSuccess) return e;
+  ws.mixed_grid_src = sms * (per_sm > 0 ? per_sm : 1);
   return cudaSuccess;
 }
 
 cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p, cudaStream_t s) {
   if (p.precision == 0)
     traverse_fp64_kernel<<<ws.fp64_grid > 0 ? ws.fp64_grid : 148, 256, 0, s>>>(ws, p);
+  else if (p.soft > 0.0)
+    traverse_mixed_kernel<false><<<ws.mixed_grid > 0 ? ws.mixed_grid : 148, kMixedWarps * 32, 0, s>>>(ws, p);
   else
-    traverse_mixed_kernel<<<ws.mixed_grid > 0 ? ws.mixed_grid : 148, kMixedWarps * 32, 0, s>>>(ws, p);
+    traverse_mixed_kernel<true><<<ws.mixed_grid_src > 0 ? ws.mixed_grid_src : 148, kMixedWarps * 32, 0, s>>>(ws, p);
   count_launches(1);
   return cudaGetLastError();
 }

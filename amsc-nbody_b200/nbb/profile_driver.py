@@ -1,0 +1,35 @@
+"""Minimal driver for profiling: one simulation, `steps` graph-replayed
+steps, per-stage times of one diagnostic force evaluation.
+
+  python amsc-nbody_b200/nbb/profile_driver.py --n 1048576 --precision mixed --steps 2
+
+Workload: the benchmark's Plummer sphere (theta 0.5, eps 0.01, dt 1e-3, G 1).
+"""
+import argparse
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+import nbb  # noqa: E402
+from nbb import ics  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--steps", type=int, default=2)
+    args = ap.parse_args()
+    prec = nbb.PRECISION_MIXED if args.precision == "mixed" else nbb.PRECISION_FP64
+    p = ics.plummer(args.n, seed=0)
+    sim = nbb.Simulation(p, nbb.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec))
+    sim.initialize()
+    sim.run(args.steps)
+    stages, st = sim.profile()
+    print({k: round(v, 4) for k, v in stages.items()}, "interactions", st.interactions,
+          "mac_tests", st.mac_tests, "groups", st.n_groups, "nodes", st.n_octree_nodes)
+
+
+if __name__ == "__main__":
+    main()
