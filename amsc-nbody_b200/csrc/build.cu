@@ -1125,6 +1125,16 @@ __global__ void __launch_bounds__(kScanThreads) group_scan_kernel(Workspace ws) 
   if (base + kScanTile >= n && threadIdx.x == 0) sc->n_tgroups = prefix + (int)total;
 }
 
+// Sorted packed pairs -> caller key / index arrays (sort-only entry point).
+__global__ void __launch_bounds__(kBlock) split_pairs_kernel(const unsigned long long *pairs, int n,
+                                                             uint32_t *keys, uint32_t *idx) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned long long pr = pairs[i];
+    keys[i] = (uint32_t)(pr >> 32);
+    idx[i] = (uint32_t)(pr & 0xffffffffu);
+  }
+}
+
 // Reference-layout keys only (no particles): used by the function-level
 // topology entry points.
 __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
@@ -1194,6 +1204,31 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   count_launches(9);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kSortPasses * 256, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)kSortPasses * ws.sort_tiles * 256, s);
+  if (e != cudaSuccess) return e;
+  int blocks = (ws.n + kBlock - 1) / kBlock;
+  const int cap = grid_for(ws, 4);
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  kd_bbox_kernel<<<blocks, kBlock, 0, s>>>(ws, 0.0, 0);
+  encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
+  unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
+  for (int p = 0; p < kSortPasses; ++p) {
+    onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
+        src, dst, ws.n, p, ws.digit_hist, ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
+    unsigned long long *t = src;
+    src = dst;
+    dst = t;
+  }
+  split_pairs_kernel<<<blocks, kBlock, 0, s>>>(src, ws.n, keys, idx);
+  count_launches(4 + kSortPasses);
   return cudaGetLastError();
 }
 

@@ -242,6 +242,10 @@ cudaError_t launch_ref_octree_traversal(const RefOctree &o, const uint32_t *idx,
 cudaError_t launch_radix_tree_only(const uint32_t *keys, int n, int *left,
                                    int *right, int *rfirst, int *rlast,
                                    int *plen, int *parent, cudaStream_t s);
+// Bounding box, Morton keys and the stable (key, index) sort alone, on a
+// workspace holding only positions, scalars, digit histograms, sort status
+// and the two pair buffers; writes the caller's key and index arrays.
+cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s);
 // Leaf groups from caller sorted keys (no particles): fills uniq / gfirst /
 // gcount / glast and n_groups.
 cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys,

@@ -228,6 +228,28 @@ int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right,
  * roofline denominator of the traversal kernels. */
 int nbb_measure_fma_tflops(int precision, double *tflops);
 
+/* ------------------------------------------------- allocation-free ---- */
+
+/* No counterpart in the reference.  Bounding box, Morton keys and their
+ * stable sorted permutation (the MortonKeys result) for callers that cannot
+ * allocate device memory: a host that owns all device memory through its own
+ * pool or budget and forbids libraries to call cudaMalloc/cudaFree.  This call
+ * allocates nothing: its scratch is one file-scope device array sized for
+ * NBB_NOALLOC_MAX_PARTICLES particles (about 4.3 MB), held by every GPU that
+ * loads the library until the process exits.  x, y, z, keys and idx are
+ * device pointers of n elements; larger n is rejected with
+ * NBB_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU (other
+ * streams, other threads) race and give wrong results.  The call synchronises
+ * the given stream before it returns.  Its errors are reported by
+ * nbb_noalloc_last_error_message(). */
+#define NBB_NOALLOC_MAX_PARTICLES (1 << 18)
+int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z,
+                            size_t n, uint32_t *keys, uint32_t *idx,
+                            void *stream);
+const char *nbb_noalloc_last_error_message(void);
+
 /* Last error of the calling thread. */
 const char *nbb_last_error_message(void);
 int nbb_last_error_code(void);
