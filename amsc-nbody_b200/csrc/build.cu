@@ -1043,11 +1043,11 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
 
 // ------------------------------------------------------ target groups ---
 
-// Target groups for the traversal: every node holding more than kGroupMax
-// particles packs its children with at most kGroupMax particles, in octant
-// (= Morton) order, greedily into runs of at most kGroupMax particles; each
+// Target groups for the traversal: every node holding more than group_max
+// particles packs its children with at most group_max particles, in octant
+// (= Morton) order, greedily into runs of at most group_max particles; each
 // run is one group.  Groups are contiguous ranges of the sorted particles,
-// never larger than kGroupMax and never wider than their parent cell, so a
+// never larger than group_max and never wider than their parent cell, so a
 // warp's targets stay spatially compact (fixed 32-particle slices of the
 // Morton order can straddle the whole system where the curve jumps).
 __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
@@ -1055,16 +1055,17 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
   if (sc->error) return;
   const int m = sc->n_nodes;
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    const int gmax = ws.group_max;
     const int np = ws.psub[node];
-    if (np <= kGroupMax) {
+    if (np <= gmax) {
       if (node == 0 && np > 0) ws.tflag[0] = 1;  // the whole system is one group
       continue;
     }
     if (ws.ocount[node] > 0) {
-      // an occupied leaf with more than kGroupMax coincident-key particles:
-      // consecutive slices of kGroupMax
+      // an occupied leaf with more than group_max coincident-key particles:
+      // consecutive slices of group_max
       const int f = ws.pfirst[node];
-      for (int k = 0; k < np; k += kGroupMax)
+      for (int k = 0; k < np; k += gmax)
         if (f + k >= 0 && f + k < ws.n) ws.tflag[f + k] = 1;
       continue;
     }
@@ -1073,11 +1074,11 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
       const int c = ws.children[(size_t)node * 8 + o];
       if (c <= 0 || c >= m) continue;
       const int cp = ws.psub[c];
-      if (cp > kGroupMax) {
+      if (cp > gmax) {
         run = 0;
         continue;
       }
-      if (run == 0 || run + cp > kGroupMax) {
+      if (run == 0 || run + cp > gmax) {
         const int f = ws.pfirst[c];
         if (f >= 0 && f < ws.n) ws.tflag[f] = 1;
         run = 0;
@@ -1123,6 +1124,19 @@ __global__ void __launch_bounds__(kScanThreads) group_scan_kernel(Workspace ws) 
     }
   }
   if (base + kScanTile >= n && threadIdx.x == 0) sc->n_tgroups = prefix + (int)total;
+}
+
+// Reset the traversal counters and target-group scan state so the groups can
+// be rebuilt with another group size on an unchanged tree.
+__global__ void retarget_reset_kernel(DevScalars *sc) {
+  if (threadIdx.x == 0) {
+    sc->work_counter = 0;
+    sc->n_tgroups = 0;
+    sc->tile_counter[6] = 0;
+    sc->interactions = 0;
+    sc->mac_tests = 0;
+    sc->stack_overflow = 0;
+  }
 }
 
 // Sorted packed pairs -> caller key / index arrays (sort-only entry point).
@@ -1229,6 +1243,20 @@ cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx
   }
   split_pairs_kernel<<<blocks, kBlock, 0, s>>>(src, ws.n, keys, idx);
   count_launches(4 + kSortPasses);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_retarget(Workspace &ws, cudaStream_t s) {
+  retarget_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
+  cudaError_t e = cudaMemsetAsync(ws.tflag, 0, (size_t)ws.n, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.scan_status + ws.scan_tiles_n + ws.scan_tiles_r, 0,
+                      sizeof(unsigned long long) * (size_t)ws.scan_tiles_n, s);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_for(ws, 8);
+  group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  count_launches(3);
   return cudaGetLastError();
 }
 

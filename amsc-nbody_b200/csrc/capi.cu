@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -277,6 +278,7 @@ int check_device(const Workspace &ws, cudaStream_t s) {
 // the rebuild; kick: second half kick fused into the traversal).
 cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, double dt, int kd,
                                   cudaStream_t s) {
+  ws.group_max = (tp.group_mode && tp.group_size > 32) ? 64 : 32;
   cudaError_t e = launch_step_reset(ws, s);
   if (e == cudaSuccess) e = launch_kd_bbox(ws, dt, kd, s);
   if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
@@ -316,6 +318,7 @@ struct nbb_sim {
   cudaGraphExec_t step_graph = nullptr;
   cudaGraph_t step_graph_def = nullptr;
   uint64_t graph_kernels = 0;
+  int tuned_group_size = 0;
 };
 
 extern "C" {
@@ -354,6 +357,8 @@ static int validate_config(const nbb_config *c) {
     return fail(NBB_ERR_INVALID_ARGUMENT, "Gravitational constant must be finite and positive");
   if (c->precision != NBB_PRECISION_FP64 && c->precision != NBB_PRECISION_MIXED)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown traversal precision");
+  if (c->group_size != 0 && c->group_size != 32 && c->group_size != 64)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "group_size must be 0 (tuned), 32 or 64");
   return NBB_OK;
 }
 
@@ -409,9 +414,73 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   tp.half_dt = 0.5 * sim->cfg.time_step;
   tp.kick = kick;
   tp.precision = sim->cfg.precision;
-  tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size : 32;
+  tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size
+                                          : (sim->tuned_group_size > 0 ? sim->tuned_group_size : 32);
   tp.group_mode = default_group_mode(tp.precision);
   return tp;
+}
+
+// Group-size autotuner of the mixed walk: on the tree of the first force
+// evaluation, time the traversal (CUDA events, best of two) for each
+// candidate warp group size (32 targets = one per lane, 64 = two per lane)
+// and keep the fastest.  The choice is cached per process for the particle
+// count's power-of-two bucket, so every simulation of that size in the
+// process uses the same size; pinning nbb_config.group_size skips tuning.
+static std::mutex g_tune_lock;
+static std::vector<std::pair<int, int>> g_tuned;  // (log2 bucket, group size)
+
+static int autotune_group_size(nbb_sim *sim) {
+  Workspace &ws = sim->ws;
+  int bucket = 0;
+  while ((1 << bucket) < ws.n && bucket < 31) ++bucket;
+  {
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    for (const auto &kv : g_tuned)
+      if (kv.first == bucket) {
+        sim->tuned_group_size = kv.second;
+        break;
+      }
+  }
+  if (sim->tuned_group_size == 0) {
+    cudaStream_t s = sim->stream;
+    cudaEvent_t e0, e1;
+    NBB_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+    NBB_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+    const int candidates[2] = {32, 64};
+    float best = 1e30f;
+    int best_size = 32;
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+      TraversalParams tp = traversal_params(sim, 0);
+      tp.group_size = candidates[c];
+      ws.group_max = candidates[c];
+      for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+        e = launch_retarget(ws, s);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess && ms < best) {
+          best = ms;
+          best_size = candidates[c];
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(e, "group-size autotuning");
+    sim->tuned_group_size = best_size;
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    g_tuned.emplace_back(bucket, best_size);
+  }
+  // the initial acceleration comes from the chosen group size
+  TraversalParams tp = traversal_params(sim, 0);
+  ws.group_max = tp.group_size > 32 ? 64 : 32;
+  NBB_CUDA(launch_retarget(ws, sim->stream), "retarget");
+  NBB_CUDA(launch_traversal(ws, tp, sim->stream), "traversal");
+  return check_device(ws, sim->stream);
 }
 
 int nbb_sim_initialize(nbb_sim *sim) {
@@ -425,10 +494,17 @@ int nbb_sim_initialize(nbb_sim *sim) {
     sim->state = nbb_sim::State::failed;
     return cuda_fail(e, "initialize");
   }
-  const int st = check_device(ws, sim->stream);
+  int st = check_device(ws, sim->stream);
   if (st) {
     sim->state = nbb_sim::State::failed;
     return st;
+  }
+  if (sim->cfg.precision == NBB_PRECISION_MIXED && sim->cfg.group_size == 0) {
+    st = autotune_group_size(sim);
+    if (st) {
+      sim->state = nbb_sim::State::failed;
+      return st;
+    }
   }
   sim->state = nbb_sim::State::ready;
   return ok();
@@ -579,6 +655,7 @@ int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats) {
   stats->n_octree_nodes = sc.n_nodes;
   stats->interactions = (int64_t)sc.interactions;
   stats->mac_tests = (int64_t)sc.mac_tests;
+  stats->group_size = sim->cfg.precision == NBB_PRECISION_MIXED ? traversal_params(sim, 0).group_size : 0;
   return ok();
 }
 
@@ -686,6 +763,7 @@ int nbb_accel(size_t n, const double *mass, const double *x, const double *y, co
     stats->n_octree_nodes = d.n_nodes;
     stats->interactions = (int64_t)d.interactions;
     stats->mac_tests = (int64_t)d.mac_tests;
+    stats->group_size = precision == NBB_PRECISION_MIXED ? tp.group_size : 0;
   }
   if (export_out) {
     st = export_workspace(ws, export_out, sc.s, true);

@@ -57,8 +57,8 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs
 constexpr int kSortPasses = 4;                        // 8-bit digits, bits 32..63
 
-// Largest target group (one target per lane of a warp).
-constexpr int kGroupMax = 32;
+// Largest target group supported (two targets per lane of a warp).
+constexpr int kGroupMaxLimit = 64;
 
 // Single-pass scan tiling.
 constexpr int kScanThreads = 256;
@@ -71,8 +71,8 @@ struct Workspace {
   int cap_nodes = 0;    // octree node capacity (sum over levels of min(8^L, n))
   int num_sms = 0;
   int fp64_grid = 0;    // persistent traversal grids (blocks)
-  int mixed_grid = 0;
-  int mixed_grid_src = 0;
+  int mixed_grid[2][2] = {{0, 0}, {0, 0}};  // [track source][targets per lane - 1]
+  int group_max = 32;   // largest octree target group (32 x targets per lane)
 
   // particle state, original order (SoA, FP64)
   double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
@@ -207,6 +207,9 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s);
 // Karras tree, plan + scan, octree materialisation, geometry, physics,
 // preorder layout.
 cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s);
+// Rebuild the octree target groups for ws.group_max on the current tree and
+// reset the traversal counters (used by the group-size autotuner).
+cudaError_t launch_retarget(Workspace &ws, cudaStream_t s);
 // Traversal (+ optional fused second half kick).
 cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p,
                              cudaStream_t s);

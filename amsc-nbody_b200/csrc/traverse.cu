@@ -82,8 +82,13 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
     int resume = valid ? 0 : INT_MAX;
     int node = __reduce_min_sync(kFull, resume);
     while (node < m) {
+      // every record of the node in one round trip (warp-uniform address:
+      // one broadcast transaction each)
+      const int4 meta = ws.node_meta[node];
+      const double4 a = ws.node_a[node];
+      const double4 c = ws.node_c[node];
+      const double4 b = ws.node_b[node];
       if (resume == node) {
-        const int4 meta = ws.node_meta[node];
         if (meta.z > 0) {
           // occupied leaf: exact sum over its particles, self excluded
           // (barnes_hut.cu:226-277)
@@ -97,31 +102,26 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
             ++inter;
           }
           resume = meta.x;
+        } else if (a.w == 0.0) {
+          resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
         } else {
-          const double4 a = ws.node_a[node];
-          if (a.w == 0.0) {
-            resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
+          const double dx = __dsub_rn(a.x, t.x), dy = __dsub_rn(a.y, t.y), dz = __dsub_rn(a.z, t.z);
+          const double d2 = sqdist(dx, dy, dz);
+          // sqrt(d2) > crit, decided on d2 vs crit^2 outside a 2^-44 band
+          bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
+          ++tests;
+          if (accept) {
+            const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w &&
+                                  fabs(__dsub_rn(t.y, b.y)) <= b.w &&
+                                  fabs(__dsub_rn(t.z, b.z)) <= b.w;
+            accept = !contains && d2 > 0.0;
+          }
+          if (accept) {
+            singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
+            ++inter;
+            resume = meta.x;
           } else {
-            const double dx = __dsub_rn(a.x, t.x), dy = __dsub_rn(a.y, t.y), dz = __dsub_rn(a.z, t.z);
-            const double d2 = sqdist(dx, dy, dz);
-            const double4 c = ws.node_c[node];
-            // sqrt(d2) > crit, decided on d2 vs crit^2 outside a 2^-44 band
-            bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
-            ++tests;
-            if (accept) {
-              const double4 b = ws.node_b[node];
-              const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w &&
-                                    fabs(__dsub_rn(t.y, b.y)) <= b.w &&
-                                    fabs(__dsub_rn(t.z, b.z)) <= b.w;
-              accept = !contains && d2 > 0.0;
-            }
-            if (accept) {
-              singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
-              ++inter;
-              resume = meta.x;
-            } else {
-              resume = node + 1;
-            }
+            resume = node + 1;
           }
         }
       }
@@ -173,60 +173,80 @@ struct MixedShared {
   int src[kMixedWarps][kTrackSource ? kListCap : 1];
 };
 
-// Evaluate `count` list entries for this lane's target: FP32 offsets, rsqrtf
-// plus one Newton step, plain FP32 partial sum over the batch, then one
-// Kahan-compensated addition of the batch partial into the running sum.
+// Evaluate `count` list entries for this lane's kTPL targets: FP32 offsets,
+// rsqrtf plus one Newton step, plain FP32 partial sums over the batch, then
+// one Kahan-compensated addition of each batch partial into its running sum.
 //
-// With positive softening the target's own entry (a leaf particle equal to
-// the target) has offset exactly (0, 0, 0) -- both offsets are rounded from
-// the same FP64 difference -- and contributes exactly zero, so no source
-// index is needed.  With zero softening the source index excludes self and
-// detects the reference's singular interaction (returns true).
-template <bool kTrackSource>
-__device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, int count, int self,
-                                           float tx, float ty, float tz, float eps2, float3 &sum,
-                                           float3 &comp) {
-  float px = 0.f, py = 0.f, pz = 0.f;
+// With positive softening a target's own entry (a leaf particle equal to the
+// target) has offset exactly (0, 0, 0) -- both offsets are rounded from the
+// same FP64 difference -- and contributes exactly zero, so no source index is
+// needed.  With zero softening the source index excludes self and detects
+// the reference's singular interaction (returns true).
+template <bool kTrackSource, int kTPL>
+__device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, int count, const int *self,
+                                           const float *tx, const float *ty, const float *tz, float eps2,
+                                           float3 *sum, float3 *comp) {
+  float px[kTPL], py[kTPL], pz[kTPL];
+#pragma unroll
+  for (int q = 0; q < kTPL; ++q) px[q] = py[q] = pz[q] = 0.f;
   bool singular = false;
 #pragma unroll 8
   for (int j = 0; j < count; ++j) {
     const float4 e = list[j];
-    const float dx = e.x - tx, dy = e.y - ty, dz = e.z - tz;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-    float r = rsqrtf(r2);
-    r = r * fmaf(-0.5f * r2, r * r, 1.5f);
-    float f = e.w * (r * r * r);
-    if (kTrackSource) {
-      const bool other = src[j] != self;
-      singular |= other && !(r2 > 0.f) && e.w != 0.f;
-      f = (other && r2 > 0.f) ? f : 0.f;
+#pragma unroll
+    for (int q = 0; q < kTPL; ++q) {
+      const float dx = e.x - tx[q], dy = e.y - ty[q], dz = e.z - tz[q];
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+      float r = rsqrtf(r2);
+      r = r * fmaf(-0.5f * r2, r * r, 1.5f);
+      float f = e.w * (r * r * r);
+      if (kTrackSource) {
+        const bool other = src[j] != self[q];
+        singular |= other && !(r2 > 0.f) && e.w != 0.f;
+        f = (other && r2 > 0.f) ? f : 0.f;
+      }
+      px[q] = fmaf(f, dx, px[q]);
+      py[q] = fmaf(f, dy, py[q]);
+      pz[q] = fmaf(f, dz, pz[q]);
     }
-    px = fmaf(f, dx, px);
-    py = fmaf(f, dy, py);
-    pz = fmaf(f, dz, pz);
   }
-  float y, t;
-  y = px - comp.x; t = sum.x + y; comp.x = (t - sum.x) - y; sum.x = t;
-  y = py - comp.y; t = sum.y + y; comp.y = (t - sum.y) - y; sum.y = t;
-  y = pz - comp.z; t = sum.z + y; comp.z = (t - sum.z) - y; sum.z = t;
+#pragma unroll
+  for (int q = 0; q < kTPL; ++q) {
+    float y, t;
+    y = px[q] - comp[q].x; t = sum[q].x + y; comp[q].x = (t - sum[q].x) - y; sum[q].x = t;
+    y = py[q] - comp[q].y; t = sum[q].y + y; comp[q].y = (t - sum[q].y) - y; sum[q].y = t;
+    y = pz[q] - comp[q].z; t = sum[q].z + y; comp[q].z = (t - sum[q].z) - y; sum[q].z = t;
+  }
   return singular;
 }
 
+// Per-lane target state of the mixed walk.
+template <int kTPL>
+struct LaneTargets {
+  int s[kTPL];
+  bool valid[kTPL];
+  float tx[kTPL], ty[kTPL], tz[kTPL];
+  float3 sum[kTPL], comp[kTPL];
+  long long inter = 0;
+  bool singular = false;
+};
+
 // Evaluate full batches of 32 from the front of the list, shifting the
 // remainder down, until fewer than 32 entries are left.
-template <bool kTrackSource>
-__device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, int self, bool valid,
-                                           float tx, float ty, float tz, float eps2, float3 &sum,
-                                           float3 &comp, long long &inter, bool &singular) {
+template <bool kTrackSource, int kTPL>
+__device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, LaneTargets<kTPL> &lt_,
+                                           float eps2) {
   const int lane = threadIdx.x & 31;
   int done = 0;
   while (ls - done >= 32) {
-    const bool sg = eval_batch<kTrackSource>(list + done, src + (kTrackSource ? done : 0), 32, self,
-                                             tx, ty, tz, eps2, sum, comp);
-    if (valid) {
-      inter += 32;
-      singular |= sg;
-    }
+    const bool sg = eval_batch<kTrackSource, kTPL>(list + done, src + (kTrackSource ? done : 0), 32, lt_.s,
+                                                   lt_.tx, lt_.ty, lt_.tz, eps2, lt_.sum, lt_.comp);
+#pragma unroll
+    for (int q = 0; q < kTPL; ++q)
+      if (lt_.valid[q]) {
+        lt_.inter += 32;
+        lt_.singular |= sg;
+      }
     done += 32;
   }
   if (done) {
@@ -241,20 +261,21 @@ __device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, int 
   }
 }
 
-// Mixed-precision traversal, one warp per target group (at most 32
-// Morton-consecutive targets inside one parent cell).  The group's bounding
-// box (FP64) replaces the target in the reference's acceptance test: a node
-// is accepted for the whole group when the box does not touch the cell and
-// the box-to-centre-of-mass distance exceeds crit = side/theta +
-// |com - centre|, which implies acceptance for every target in the box.
-// Nodes are examined 32 at a time (one per lane) from a warp-private stack
-// in shared memory, each lane fetching its node's record and child list in
-// one round trip; accepted nodes and the particles of reached leaves go to a
-// shared interaction list as FP32 offsets from the group centre (formed in
-// FP64, then rounded) and are evaluated by all lanes in batches of 32.
-template <bool kTrackSource>
+// Mixed-precision traversal, one warp per target group of at most 32 x kTPL
+// Morton-consecutive targets inside one parent cell (kTPL targets per lane).
+// The group's bounding box (FP64) replaces the target in the reference's
+// acceptance test: a node is accepted for the whole group when the box does
+// not touch the cell and the box-to-centre-of-mass distance exceeds
+// crit = side/theta + |com - centre|, which implies acceptance for every
+// target in the box.  Nodes are examined 32 at a time (one per lane) from a
+// warp-private stack in shared memory, each lane fetching its node's record
+// and child list in one round trip; accepted nodes and the particles of
+// reached leaves go to a shared interaction list as FP32 offsets from the
+// group centre (formed in FP64, then rounded) and are evaluated by all lanes
+// in batches of 32.
+template <bool kTrackSource, int kTPL>
 __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) traverse_mixed_kernel(Workspace ws,
-                                                                          TraversalParams p) {
+                                                                                            TraversalParams p) {
   __shared__ MixedShared<kTrackSource> sh;
   DevScalars *sc = ws.sc;
   if (sc->error) return;
@@ -265,23 +286,40 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
   int *src = sh.src[wid];
   const int n = ws.n;
   const int m = sc->n_nodes;
-  const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
+  const int n_groups = p.group_mode ? sc->n_tgroups : (n + 32 * kTPL - 1) / (32 * kTPL);
   const float eps2 = (float)(p.soft * p.soft);
   const unsigned lt = lanemask_lt();
-  long long inter = 0, tests = 0;
+  long long tests = 0;
   unsigned overflow = 0;
-  bool singular = false;
+  long long inter_total = 0;
+  bool singular_any = false;
   while (true) {
     int grp = 0;
     if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
     grp = __shfl_sync(kFull, grp, 0);
     if (grp >= n_groups) break;
-    const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
-    const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
-    const int s = g0 + lane;
-    const bool valid = s < g1 && s < n;
-    const double4 t = ws.pm4[valid ? s : g0];
-    double lo[3] = {t.x, t.y, t.z}, hi[3] = {t.x, t.y, t.z};
+    const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32 * kTPL;
+    const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32 * kTPL, n);
+    LaneTargets<kTPL> T;
+    double4 tp[kTPL];
+    double lo[3], hi[3];
+#pragma unroll
+    for (int q = 0; q < kTPL; ++q) {
+      T.s[q] = g0 + lane + 32 * q;
+      T.valid[q] = T.s[q] < g1 && T.s[q] < n;
+      tp[q] = ws.pm4[T.valid[q] ? T.s[q] : g0];
+      T.sum[q] = make_float3(0.f, 0.f, 0.f);
+      T.comp[q] = make_float3(0.f, 0.f, 0.f);
+    }
+    lo[0] = hi[0] = tp[0].x;
+    lo[1] = hi[1] = tp[0].y;
+    lo[2] = hi[2] = tp[0].z;
+#pragma unroll
+    for (int q = 1; q < kTPL; ++q) {
+      lo[0] = fmin(lo[0], tp[q].x); hi[0] = fmax(hi[0], tp[q].x);
+      lo[1] = fmin(lo[1], tp[q].y); hi[1] = fmax(hi[1], tp[q].y);
+      lo[2] = fmin(lo[2], tp[q].z); hi[2] = fmax(hi[2], tp[q].z);
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       for (int o = 16; o > 0; o >>= 1) {
@@ -291,8 +329,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
     }
     const double gcx = 0.5 * (lo[0] + hi[0]), gcy = 0.5 * (lo[1] + hi[1]),
                  gcz = 0.5 * (lo[2] + hi[2]);
-    const float tx = (float)(t.x - gcx), ty = (float)(t.y - gcy), tz = (float)(t.z - gcz);
-    float3 sum = make_float3(0.f, 0.f, 0.f), comp = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < kTPL; ++q) {
+      T.tx[q] = (float)(tp[q].x - gcx);
+      T.ty[q] = (float)(tp[q].y - gcy);
+      T.tz[q] = (float)(tp[q].z - gcz);
+    }
     int ls = 0;
     if (lane == 0) stack[0] = 0;
     int sp = (m > 0) ? 1 : 0;
@@ -383,10 +425,10 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
         }
         ls += ltotal;
         __syncwarp();
-        flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
       } else {
         __syncwarp();
-        flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
         unsigned lm = __ballot_sync(kFull, cat == 2);
         while (lm) {
           const int l = __ffs(lm) - 1;
@@ -402,24 +444,28 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
             }
             ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
             __syncwarp();
-            flush_full<kTrackSource>(list, src, ls, s, valid, tx, ty, tz, eps2, sum, comp, inter, singular);
+            flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
           }
         }
       }
     }
     if (ls > 0) {
-      const bool sg = eval_batch<kTrackSource>(list, src, ls, s, tx, ty, tz, eps2, sum, comp);
-      if (valid) {
-        inter += ls;
-        singular |= sg;
-      }
+      const bool sg = eval_batch<kTrackSource, kTPL>(list, src, ls, T.s, T.tx, T.ty, T.tz, eps2, T.sum, T.comp);
+#pragma unroll
+      for (int q = 0; q < kTPL; ++q)
+        if (T.valid[q]) {
+          T.inter += ls;
+          T.singular |= sg;
+        }
     }
     __syncwarp();
-    if (valid) {
-      const double ax = p.g * ((double)sum.x - (double)comp.x);
-      const double ay = p.g * ((double)sum.y - (double)comp.y);
-      const double az = p.g * ((double)sum.z - (double)comp.z);
-      const uint32_t ti = ws.idx[s];
+#pragma unroll
+    for (int q = 0; q < kTPL; ++q) {
+      if (!T.valid[q]) continue;
+      const double ax = p.g * ((double)T.sum[q].x - (double)T.comp[q].x);
+      const double ay = p.g * ((double)T.sum[q].y - (double)T.comp[q].y);
+      const double az = p.g * ((double)T.sum[q].z - (double)T.comp[q].z);
+      const uint32_t ti = ws.idx[T.s[q]];
       ws.ax[ti] = ax;
       ws.ay[ti] = ay;
       ws.az[ti] = az;
@@ -429,14 +475,16 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
         ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
       }
     }
+    inter_total += T.inter;
+    singular_any |= T.singular;
   }
-  if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
-  inter = warp_sum_ll(inter);
+  if (__any_sync(kFull, singular_any) && lane == 0) record_error(sc, kStageTraversal, 6);
+  inter_total = warp_sum_ll(inter_total);
   tests = warp_sum_ll(tests);
   unsigned ov = overflow;
   for (int o = 16; o > 0; o >>= 1) ov += __shfl_xor_sync(kFull, ov, o);
   if (lane == 0) {
-    atomicAdd(&sc->interactions, (unsigned long long)inter);
+    atomicAdd(&sc->interactions, (unsigned long long)inter_total);
     atomicAdd(&sc->mac_tests, (unsigned long long)tests);
     if (ov) atomicAdd(&sc->stack_overflow, ov);
   }
@@ -699,28 +747,38 @@ int device_sms() {
 
 // Persistent grids: as many resident blocks as the occupancy calculator
 // allows on every SM; warps then pull target groups from a work counter.
+template <typename K>
+static cudaError_t grid_of(K kernel, int threads, int sms, int &grid) {
+  int per_sm = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+  grid = sms * (per_sm > 0 ? per_sm : 1);
+  return e;
+}
+
 cudaError_t configure_traversal(Workspace &ws) {
   const int sms = ws.num_sms > 0 ? ws.num_sms : 148;
-  int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_fp64_kernel, 256, 0);
-  if (e != cudaSuccess) return e;
-  ws.fp64_grid = sms * (per_sm > 0 ? per_sm : 1);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel<false>, kMixedWarps * 32, 0);
-  if (e != cudaSuccess) return e;
-  ws.mixed_grid = sms * (per_sm > 0 ? per_sm : 1);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_mixed_kernel<true>, kMixedWarps * 32, 0);
-  if (e != cudaSuccess) return e;
-  ws.mixed_grid_src = sms * (per_sm > 0 ? per_sm : 1);
-  return cudaSuccess;
+  cudaError_t e = grid_of(traverse_fp64_kernel, 256, sms, ws.fp64_grid);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 1>, kMixedWarps * 32, sms, ws.mixed_grid[0][0]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 1>, kMixedWarps * 32, sms, ws.mixed_grid[1][0]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 2>, kMixedWarps * 32, sms, ws.mixed_grid[0][1]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 2>, kMixedWarps * 32, sms, ws.mixed_grid[1][1]);
+  return e;
 }
 
 cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p, cudaStream_t s) {
+  const int tpl = (p.group_mode && p.group_size > 32) ? 2 : 1;
+  const int track = p.soft > 0.0 ? 0 : 1;
+  const int grid = ws.mixed_grid[track][tpl - 1] > 0 ? ws.mixed_grid[track][tpl - 1] : 148;
   if (p.precision == 0)
     traverse_fp64_kernel<<<ws.fp64_grid > 0 ? ws.fp64_grid : 148, 256, 0, s>>>(ws, p);
-  else if (p.soft > 0.0)
-    traverse_mixed_kernel<false><<<ws.mixed_grid > 0 ? ws.mixed_grid : 148, kMixedWarps * 32, 0, s>>>(ws, p);
+  else if (!track && tpl == 1)
+    traverse_mixed_kernel<false, 1><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+  else if (track && tpl == 1)
+    traverse_mixed_kernel<true, 1><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+  else if (!track)
+    traverse_mixed_kernel<false, 2><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
   else
-    traverse_mixed_kernel<true><<<ws.mixed_grid_src > 0 ? ws.mixed_grid_src : 148, kMixedWarps * 32, 0, s>>>(ws, p);
+    traverse_mixed_kernel<true, 2><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
   count_launches(1);
   return cudaGetLastError();
 }

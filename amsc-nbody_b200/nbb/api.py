@@ -196,7 +196,7 @@ def _export(call, n: int, m_capacity: int | None = None, fields=None) -> dict:
 
 def compute_accelerations(particles_or_arrays, theta: float, softening: float, g: float = 1.0,
                           precision: int = _lib.PRECISION_FP64, export: bool = False,
-                          stats: bool = False):
+                          stats: bool = False):  # noqa: D417
     """One rebuild + Barnes-Hut evaluation of caller particles (host arrays):
     the reference's pipeline of src/simulation.cpp:353-414 with an explicit
     G.  Returns (ax, ay, az) [, export dict] [, Stats]."""

@@ -128,6 +128,7 @@ typedef struct {
   int n_octree_nodes;   /* M */
   int64_t interactions; /* monopole + leaf-pair interactions evaluated */
   int64_t mac_tests;    /* acceptance tests evaluated */
+  int group_size;       /* MIXED: warp target group size in use (32 or 64) */
 } nbb_stats;
 int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats);
 

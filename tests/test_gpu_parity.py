@@ -377,6 +377,41 @@ def test_mixed_force_error(nbb_mod, recipe, n, theta, soft):
         assert rms_mixed <= MIXED_RMS_BOUND, rms_mixed
 
 
+@pytest.mark.parametrize("group_size", [32, 64])
+def test_mixed_group_sizes(nbb_mod, group_size):
+    """Both warp group sizes (one or two targets per lane) stay within the
+    headline bound and match each other to the Barnes-Hut error level."""
+    from nbb import ics
+
+    n = 65536
+    p = ics.plummer(n, seed=0)
+    rng = np.random.Generator(np.random.Philox(99))
+    tg = np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32)
+    exact = np.stack(nbb_mod.compute_direct_accelerations(p.mass, p.x, p.y, p.z, 1.0, 0.01, targets=tg))
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0,
+                                                         precision=nbb_mod.PRECISION_MIXED,
+                                                         group_size=group_size))
+    sim.initialize()
+    assert sim.stats().group_size == group_size
+    a = np.stack(sim.accelerations())[:, tg]
+    assert _rms_rel(a, exact) <= MIXED_RMS_BOUND
+
+
+def test_mixed_autotuned_group_size(nbb_mod):
+    from nbb import ics
+
+    p = ics.plummer(32768, seed=1)
+    sizes = []
+    for _ in range(2):
+        sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0,
+                                                             precision=nbb_mod.PRECISION_MIXED))
+        sim.initialize()
+        sizes.append(sim.stats().group_size)
+    assert sizes[0] in (32, 64) and sizes[0] == sizes[1]  # cached per process and size
+    with pytest.raises(nbb_mod.InvalidArgument):
+        nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, group_size=48))
+
+
 def test_mixed_theta_zero_is_direct(nbb_mod):
     from nbb import ics
 
