@@ -253,7 +253,7 @@ def run_nbb(args, rank, world, local):
         results[name] = {"ms_per_step": total_ms / args.steps, "step_ms": times, "launches": launches,
                          "stages_ms": stage_ms, "interactions": st.interactions,
                          "mac_tests": st.mac_tests, "n_groups": st.n_groups,
-                         "n_octree_nodes": st.n_octree_nodes}
+                         "n_octree_nodes": st.n_octree_nodes, "group_size": st.group_size}
     # end to end through the public API: pinned host state in, step, state out
     sim = sims["mixed"]
     pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in p.arrays()]
@@ -285,6 +285,32 @@ class _Null:
 
     def __exit__(self, *exc):
         return False
+
+
+# Algorithmic bytes of the rebuild (the minimum each stage must move), per
+# particle, per unique-key group, per radix node and per octree node; the
+# derivation is tabulated in DESIGN.md.
+BUILD_BYTES_PER_PARTICLE = 120 + 32 + 64 + 80 + 32  # KD+bbox, encode, 4 sort passes, groups+gather, leaf mass
+BUILD_BYTES_PER_GROUP = 12 + 28                     # group arrays, Karras internal node
+BUILD_BYTES_PER_RADIX_NODE = 20 + 40                # plan + scan, materialise
+BUILD_BYTES_PER_OCTREE_NODE = 108 + 78 + 100 + 224  # clear, geometry/child count, propagate, layout
+
+
+def build_algorithmic_bytes(n, groups, nodes):
+    return (BUILD_BYTES_PER_PARTICLE * n + BUILD_BYTES_PER_GROUP * groups
+            + BUILD_BYTES_PER_RADIX_NODE * (2 * groups - 1) + BUILD_BYTES_PER_OCTREE_NODE * nodes)
+
+
+def profiled_traffic(kernel_file):
+    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", kernel_file)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def load_peaks():
@@ -357,7 +383,10 @@ def bench_nbb(args, rank, world, local):
     peak64 = nbb.measure_fma_tflops(nbb.PRECISION_FP64)
     sm_mhz = clocks.get("sm_max_mhz") or 1965.0
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
-                        "frac": achieved / peak32, "traffic": None,
+                        "frac": achieved / peak32,
+                        "traffic": profiled_traffic("traverse_mixed_plummer_2e20.md"),
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                          "launch (profiles/traverse_mixed_plummer_2e20.md)",
                         "kernel": "traverse_mixed_kernel",
                         "peak_source": "measured in this run: SIMT FP32 FMA throughput kernel "
                                        "(MEASURED_PEAKS.json has HBM and bf16-tensor figures only; "
@@ -372,9 +401,15 @@ def bench_nbb(args, rank, world, local):
                                       "interactions_per_s": plain["interactions"] / (ptrav * 1e-3)}
     peaks = load_peaks()
     hbm = peaks.get("hbm_gbs")
-    if hbm:
-        # build stages are HBM-bound: bytes per particle per step
-        line["roofline"]["hbm_gbs_measured_peak"] = hbm
+    st = mixed["stages_ms"]
+    build_ms = st["bbox"] + st["morton_sort_groups"] + st["tree"]
+    build_bytes = build_algorithmic_bytes(args.n, mixed["n_groups"], mixed["n_octree_nodes"])
+    build_gbs = build_bytes / (build_ms * 1e-3) / 1e9
+    line["build_roofline"] = {"bound": "hbm", "achieved": build_gbs, "peak": hbm, "unit": "GB/s",
+                              "frac": (build_gbs / hbm) if hbm else None,
+                              "algorithmic_bytes": build_bytes, "ms": build_ms,
+                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+    line["group_size"] = mixed["group_size"]
     if rank == 0 and not args.no_error:
         rng = np.random.Generator(np.random.Philox(12345))
         tg = np.sort(rng.choice(args.n, min(ERROR_TARGETS, args.n), replace=False)).astype(np.int32)
