@@ -38,6 +38,11 @@ inline int grid_for(const Workspace &ws, int per_sm = 8) {
 
 // ------------------------------------------------------------- reset ----
 
+__global__ void reset_sys_kernel(unsigned long long *bb, int n_systems) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 6 * n_systems; k += gridDim.x * blockDim.x)
+    bb[k] = (k % 6 < 3) ? ~0ull : 0ull;
+}
+
 __global__ void reset_scalars_kernel(DevScalars *sc) {
   if (threadIdx.x == 0) {
     for (int a = 0; a < 3; ++a) {
@@ -71,64 +76,119 @@ __device__ __forceinline__ T warp_reduce_max(T v) {
   return v;
 }
 
+// Box of one system from its encoded extrema (globalbounding.cu:158-172):
+// centre = (min + max) * 0.5, side = 1.1 * longest extent, 1 when that is 0.
+__device__ void finish_box(const unsigned long long *mn, const unsigned long long *mx, double *box) {
+  double lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = order_value(mn[a]);
+    hi[a] = order_value(mx[a]);
+  }
+  for (int a = 0; a < 3; ++a) box[a] = __dmul_rn(__dadd_rn(lo[a], hi[a]), 0.5);
+  double ext = __dsub_rn(hi[0], lo[0]);
+  const double ey = __dsub_rn(hi[1], lo[1]);
+  const double ez = __dsub_rn(hi[2], lo[2]);
+  if (ey > ext) ext = ey;
+  if (ez > ext) ext = ez;
+  double side = __dmul_rn(1.1, ext);
+  if (side == 0.0) side = 1.0;
+  box[3] = side;
+}
+
 // One pass over the state: optional first half kick + drift
 // (integrator.cu:57-89), then the extrema of the new positions and a
-// non-finite flag (globalbounding.cu:62-92).  The last block to finish forms
-// centre = (min + max) * 0.5 and side = 1.1 * longest extent, or 1 when that
-// is 0 (globalbounding.cu:158-172).
+// non-finite flag (globalbounding.cu:62-92), per system.  The last block to
+// finish forms every system's box.  A single system reduces through shared
+// memory with one set of atomics per block; an ensemble (systems stored
+// contiguously) reduces per warp when the warp's particles share a system
+// and per particle otherwise.
 __global__ void __launch_bounds__(kBlock) kd_bbox_kernel(Workspace ws, double dt,
                                                          int do_kd) {
   __shared__ double s_lo[3][kBlock / 32], s_hi[3][kBlock / 32];
   __shared__ int s_nf[kBlock / 32];
   __shared__ bool s_last;
   const int n = ws.n;
+  const bool multi = ws.n_systems > 1;
   const double hdt = 0.5 * dt;
   double lo0 = INFINITY, lo1 = INFINITY, lo2 = INFINITY;
   double hi0 = -INFINITY, hi1 = -INFINITY, hi2 = -INFINITY;
   int nf = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    double px = ws.x[i], py = ws.y[i], pz = ws.z[i];
-    if (do_kd) {
-      const double vx = __fma_rn(hdt, ws.ax[i], ws.vx[i]);
-      const double vy = __fma_rn(hdt, ws.ay[i], ws.vy[i]);
-      const double vz = __fma_rn(hdt, ws.az[i], ws.vz[i]);
-      ws.vx[i] = vx;
-      ws.vy[i] = vy;
-      ws.vz[i] = vz;
-      px = __fma_rn(dt, vx, px);
-      py = __fma_rn(dt, vy, py);
-      pz = __fma_rn(dt, vz, pz);
-      ws.x[i] = px;
-      ws.y[i] = py;
-      ws.z[i] = pz;
+  DevScalars *sc = ws.sc;
+  const int lane = threadIdx.x & 31;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int i = base + threadIdx.x;
+    const bool in = i < n;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    if (in) {
+      px = ws.x[i];
+      py = ws.y[i];
+      pz = ws.z[i];
+      if (do_kd) {
+        const double vx = __fma_rn(hdt, ws.ax[i], ws.vx[i]);
+        const double vy = __fma_rn(hdt, ws.ay[i], ws.vy[i]);
+        const double vz = __fma_rn(hdt, ws.az[i], ws.vz[i]);
+        ws.vx[i] = vx;
+        ws.vy[i] = vy;
+        ws.vz[i] = vz;
+        px = __fma_rn(dt, vx, px);
+        py = __fma_rn(dt, vy, py);
+        pz = __fma_rn(dt, vz, pz);
+        ws.x[i] = px;
+        ws.y[i] = py;
+        ws.z[i] = pz;
+      }
+      nf |= !(isfinite(px) && isfinite(py) && isfinite(pz));
     }
-    nf |= !(isfinite(px) && isfinite(py) && isfinite(pz));
-    lo0 = fmin(lo0, px); hi0 = fmax(hi0, px);
-    lo1 = fmin(lo1, py); hi1 = fmax(hi1, py);
-    lo2 = fmin(lo2, pz); hi2 = fmax(hi2, pz);
+    if (!multi) {
+      if (in) {
+        lo0 = fmin(lo0, px); hi0 = fmax(hi0, px);
+        lo1 = fmin(lo1, py); hi1 = fmax(hi1, py);
+        lo2 = fmin(lo2, pz); hi2 = fmax(hi2, pz);
+      }
+      continue;
+    }
+    // ensemble: per-system extrema
+    const int sys = in ? ws.sys_of[i] : -1;
+    const int sys0 = __shfl_sync(0xffffffffu, sys, 0);
+    const bool uniform = __all_sync(0xffffffffu, !in || sys == sys0) && sys0 >= 0;
+    double l0 = in ? px : INFINITY, l1 = in ? py : INFINITY, l2 = in ? pz : INFINITY;
+    double h0 = in ? px : -INFINITY, h1 = in ? py : -INFINITY, h2 = in ? pz : -INFINITY;
+    if (uniform) {
+      l0 = warp_reduce_min(l0); l1 = warp_reduce_min(l1); l2 = warp_reduce_min(l2);
+      h0 = warp_reduce_max(h0); h1 = warp_reduce_max(h1); h2 = warp_reduce_max(h2);
+    }
+    if (in && (!uniform || lane == 0)) {
+      unsigned long long *b = ws.sys_bb + 6 * (size_t)sys;
+      atomicMin(b + 0, order_bits(l0)); atomicMax(b + 3, order_bits(h0));
+      atomicMin(b + 1, order_bits(l1)); atomicMax(b + 4, order_bits(h1));
+      atomicMin(b + 2, order_bits(l2)); atomicMax(b + 5, order_bits(h2));
+    }
   }
-  lo0 = warp_reduce_min(lo0); lo1 = warp_reduce_min(lo1); lo2 = warp_reduce_min(lo2);
-  hi0 = warp_reduce_max(hi0); hi1 = warp_reduce_max(hi1); hi2 = warp_reduce_max(hi2);
   nf = __any_sync(0xffffffffu, nf);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) {
-    s_lo[0][warp] = lo0; s_lo[1][warp] = lo1; s_lo[2][warp] = lo2;
-    s_hi[0][warp] = hi0; s_hi[1][warp] = hi1; s_hi[2][warp] = hi2;
-    s_nf[warp] = nf;
+  const int warp = threadIdx.x >> 5;
+  if (!multi) {
+    lo0 = warp_reduce_min(lo0); lo1 = warp_reduce_min(lo1); lo2 = warp_reduce_min(lo2);
+    hi0 = warp_reduce_max(hi0); hi1 = warp_reduce_max(hi1); hi2 = warp_reduce_max(hi2);
+    if (lane == 0) {
+      s_lo[0][warp] = lo0; s_lo[1][warp] = lo1; s_lo[2][warp] = lo2;
+      s_hi[0][warp] = hi0; s_hi[1][warp] = hi1; s_hi[2][warp] = hi2;
+    }
   }
+  if (lane == 0) s_nf[warp] = nf;
   __syncthreads();
   if (threadIdx.x == 0) {
-    DevScalars *sc = ws.sc;
     int anynf = 0;
-    for (int a = 0; a < 3; ++a) {
-      double lo = INFINITY, hi = -INFINITY;
-      for (int w = 0; w < kBlock / 32; ++w) {
-        lo = fmin(lo, s_lo[a][w]);
-        hi = fmax(hi, s_hi[a][w]);
-      }
-      if (lo <= hi) {
-        atomicMin(&sc->bb_min[a], order_bits(lo));
-        atomicMax(&sc->bb_max[a], order_bits(hi));
+    if (!multi) {
+      for (int a = 0; a < 3; ++a) {
+        double lo = INFINITY, hi = -INFINITY;
+        for (int w = 0; w < kBlock / 32; ++w) {
+          lo = fmin(lo, s_lo[a][w]);
+          hi = fmax(hi, s_hi[a][w]);
+        }
+        if (lo <= hi) {
+          atomicMin(&ws.sys_bb[a], order_bits(lo));
+          atomicMax(&ws.sys_bb[3 + a], order_bits(hi));
+        }
       }
     }
     for (int w = 0; w < kBlock / 32; ++w) anynf |= s_nf[w];
@@ -138,25 +198,19 @@ __global__ void __launch_bounds__(kBlock) kd_bbox_kernel(Workspace ws, double dt
     s_last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
+  if (s_last) {
     __threadfence();
-    DevScalars *sc = ws.sc;
-    double lo[3], hi[3];
-    for (int a = 0; a < 3; ++a) {
-      lo[a] = order_value(atomicAdd(&sc->bb_min[a], 0ull));
-      hi[a] = order_value(atomicAdd(&sc->bb_max[a], 0ull));
+    if (threadIdx.x == 0 && atomicAdd(&sc->nonfinite, 0)) record_error(sc, kStageBbox, 1);
+    for (int sys = threadIdx.x; sys < ws.n_systems; sys += blockDim.x) {
+      unsigned long long mn[3], mx[3];
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = atomicAdd(&ws.sys_bb[6 * (size_t)sys + a], 0ull);
+        mx[a] = atomicAdd(&ws.sys_bb[6 * (size_t)sys + 3 + a], 0ull);
+      }
+      finish_box(mn, mx, ws.sys_box + 4 * (size_t)sys);
+      if (sys == 0)
+        for (int a = 0; a < 4; ++a) sc->box[a] = ws.sys_box[a];
     }
-    const int bad = atomicAdd(&sc->nonfinite, 0);
-    if (bad) record_error(sc, kStageBbox, 1);
-    for (int a = 0; a < 3; ++a) sc->box[a] = __dmul_rn(__dadd_rn(lo[a], hi[a]), 0.5);
-    double ext = __dsub_rn(hi[0], lo[0]);
-    const double ey = __dsub_rn(hi[1], lo[1]);
-    const double ez = __dsub_rn(hi[2], lo[2]);
-    if (ey > ext) ext = ey;
-    if (ez > ext) ext = ez;
-    double side = __dmul_rn(1.1, ext);
-    if (side == 0.0) side = 1.0;
-    sc->box[3] = side;
   }
 }
 
@@ -182,37 +236,50 @@ __device__ __forceinline__ uint32_t quantise(double a, double lower, double side
   return (uint32_t)clamped;
 }
 
-// Keys and packed (key << 32 | index) pairs, plus the 4 x 256 digit
+// Keys and packed (key << pack_shift | index) pairs, plus the digit
 // histograms of the sort passes; the last block turns the histograms into
-// exclusive digit offsets.
+// exclusive digit offsets.  An ensemble's key carries the system id above the
+// 30 Morton bits, each system quantised against its own box.
 __global__ void __launch_bounds__(kBlock) encode_kernel(Workspace ws) {
-  __shared__ uint32_t hist[kSortPasses][256];
+  __shared__ uint32_t hist[kMaxSortPasses][256];
   __shared__ bool s_last;
-  for (int k = threadIdx.x; k < kSortPasses * 256; k += blockDim.x) (&hist[0][0])[k] = 0;
+  const int passes = ws.sort_passes;
+  for (int k = threadIdx.x; k < kMaxSortPasses * 256; k += blockDim.x) (&hist[0][0])[k] = 0;
   __syncthreads();
   DevScalars *sc = ws.sc;
-  const double cxx = sc->box[0], cyy = sc->box[1], czz = sc->box[2], side = sc->box[3];
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    // morton.cu:218-219
-    if (!isfinite(cxx) || !isfinite(cyy) || !isfinite(czz) || !isfinite(side) || side <= 0.0)
-      record_error(sc, kStageBbox, 2);
-  }
-  const double half_side = __dmul_rn(side, 0.5);  // side / 2.0, exact
-  const double lx = __dsub_rn(cxx, half_side);
-  const double ly = __dsub_rn(cyy, half_side);
-  const double lz = __dsub_rn(czz, half_side);
   const int n = ws.n;
+  const bool multi = ws.n_systems > 1;
+  if (blockIdx.x == 0) {
+    // morton.cu:218-219, every system's box
+    for (int sys = threadIdx.x; sys < ws.n_systems; sys += blockDim.x) {
+      const double *b = ws.sys_box + 4 * (size_t)sys;
+      if (!isfinite(b[0]) || !isfinite(b[1]) || !isfinite(b[2]) || !isfinite(b[3]) || b[3] <= 0.0)
+        record_error(sc, kStageBbox, 2);
+    }
+  }
+  int cur = -1;
+  double lx = 0.0, ly = 0.0, lz = 0.0, side = 1.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int sys = multi ? ws.sys_of[i] : 0;
+    if (sys != cur) {
+      const double *b = ws.sys_box + 4 * (size_t)sys;
+      side = b[3];
+      const double half_side = __dmul_rn(side, 0.5);  // side / 2.0, exact
+      lx = __dsub_rn(b[0], half_side);
+      ly = __dsub_rn(b[1], half_side);
+      lz = __dsub_rn(b[2], half_side);
+      cur = sys;
+    }
     const uint32_t qx = quantise(ws.x[i], lx, side);
     const uint32_t qy = quantise(ws.y[i], ly, side);
     const uint32_t qz = quantise(ws.z[i], lz, side);
-    const uint32_t key = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
-    ws.pairs_a[i] = ((unsigned long long)key << 32) | (unsigned)i;
-#pragma unroll
-    for (int p = 0; p < kSortPasses; ++p) atomicAdd(&hist[p][(key >> (8 * p)) & 255u], 1u);
+    const unsigned long long key = ((unsigned long long)sys << kSpatialBits) |
+                                   ((expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz));
+    ws.pairs_a[i] = (key << ws.pack_shift) | (unsigned long long)i;
+    for (int p = 0; p < passes; ++p) atomicAdd(&hist[p][(key >> (8 * p)) & 255u], 1u);
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < kSortPasses * 256; k += blockDim.x) {
+  for (int k = threadIdx.x; k < passes * 256; k += blockDim.x) {
     const uint32_t c = (&hist[0][0])[k];
     if (c) atomicAdd(&ws.digit_hist[k], c);
   }
@@ -222,7 +289,7 @@ __global__ void __launch_bounds__(kBlock) encode_kernel(Workspace ws) {
   __syncthreads();
   if (s_last) {
     __threadfence();
-    if (threadIdx.x < kSortPasses) {
+    if (threadIdx.x < passes) {
       uint32_t *h = ws.digit_hist + threadIdx.x * 256;
       uint32_t run = 0;
       for (int d = 0; d < 256; ++d) {
@@ -248,7 +315,7 @@ constexpr uint32_t kDigitMask = (1u << 30) - 1u;
 // from an atomic counter, so every predecessor is already running).
 __global__ void __launch_bounds__(kSortThreads)
     onesweep_kernel(const unsigned long long *__restrict__ in,
-                    unsigned long long *__restrict__ out, int n, int pass,
+                    unsigned long long *__restrict__ out, int n, int pass, int shift,
                     const uint32_t *__restrict__ digit_offsets,
                     uint32_t *status, DevScalars *sc) {
   constexpr int kWarps = kSortThreads / 32;
@@ -260,7 +327,6 @@ __global__ void __launch_bounds__(kSortThreads)
   for (int k = tid; k < kWarps * 256; k += kSortThreads) (&whist[0][0])[k] = 0;
   __syncthreads();
   const int tile = s_tile;
-  const int shift = 32 + 8 * pass;
   const int start = tile * kSortTile + warp * (32 * kSortItems);
   unsigned long long key[kSortItems];
   uint32_t rank[kSortItems];
@@ -439,28 +505,30 @@ __device__ unsigned long long block_scan_rows(const int (&val)[ITEMS], int (&exc
 // number of flags before it.  Also splits the packed pairs into the
 // reference's key / index arrays and gathers {x, y, z, m} into Morton order.
 __global__ void __launch_bounds__(kScanThreads) groups_kernel(Workspace ws,
+                                                              const unsigned long long *pairs,
                                                               int gather) {
   __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
   __shared__ unsigned long long s_total, s_prefix;
   __shared__ int s_tile;
   DevScalars *sc = ws.sc;
   const int n = ws.n;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[4], 1u);
+  const int shift = ws.pack_shift;
+  const unsigned long long imask = (1ull << shift) - 1ull;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[kTileGroups], 1u);
   __syncthreads();
   const int tile = s_tile;
   const int base = tile * kScanTile;
   if (base >= n) return;
-  const unsigned long long *pairs = ws.pairs_a;
   int flag[kScanItems], excl[kScanItems];
-  uint32_t key[kScanItems];
+  unsigned long long key[kScanItems];
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
     const int i = base + k * kScanThreads + threadIdx.x;
     flag[k] = 0;
     key[k] = 0;
     if (i < n) {
-      key[k] = (uint32_t)(pairs[i] >> 32);
-      flag[k] = (i == 0) || (key[k] != (uint32_t)(pairs[i - 1] >> 32));
+      key[k] = pairs[i] >> shift;
+      flag[k] = (i == 0) || (key[k] != (pairs[i - 1] >> shift));
     }
   }
   const unsigned long long total = block_scan_rows<kScanItems, kScanThreads>(flag, excl, row_warp, &s_total);
@@ -476,19 +544,21 @@ __global__ void __launch_bounds__(kScanThreads) groups_kernel(Workspace ws,
     if (i >= n) continue;
     const int g = prefix + excl[k] + flag[k] - 1;
     const unsigned long long pr = pairs[i];
-    const uint32_t id = (uint32_t)(pr & 0xffffffffu);
-    if (g < 0 || g >= n || id >= (uint32_t)n) {
+    const unsigned long long id = pr & imask;
+    if (g < 0 || g >= n || id >= (unsigned long long)n) {
       record_error(sc, kStageGroups, 1);
       continue;
     }
     if (flag[k]) {
-      ws.uniq[g] = key[k];
+      ws.ukey[g] = key[k];
+      ws.uniq[g] = (uint32_t)key[k];
       ws.gfirst[g] = i;
     }
-    const bool last = (i == n - 1) || ((uint32_t)(pairs[i + 1] >> 32) != key[k]);
+    const bool last = (i == n - 1) || ((pairs[i + 1] >> shift) != key[k]);
     if (last) ws.glast[g] = i;
-    ws.keys[i] = key[k];
-    ws.idx[i] = id;
+    ws.keys[i] = (uint32_t)key[k];
+    ws.idx[i] = (uint32_t)id;
+    ws.psys[i] = (int)(key[k] >> kSpatialBits);
     if (gather) ws.pm4[i] = make_double4(ws.x[id], ws.y[id], ws.z[id], ws.m[id]);
   }
   if (base + kScanTile >= n && threadIdx.x == 0) sc->n_groups = prefix + (int)total;
@@ -496,17 +566,21 @@ __global__ void __launch_bounds__(kScanThreads) groups_kernel(Workspace ws,
 
 // ------------------------------------------------------------ Karras ----
 
-// tree_builder.cu:9-24
-__device__ __forceinline__ int lcp(const uint32_t *keys, int i, int j, int n) {
+// tree_builder.cu:9-24, for 32-bit keys (the reference's) and for 64-bit
+// keys; the 64-bit frame is the 32-bit one plus 32 for keys below 2^32.
+template <typename K>
+__device__ __forceinline__ int lcp(const K *keys, int i, int j, int n) {
   if (j < 0 || j >= n) return -1;
-  if (i == j) return 64;
-  const uint32_t a = keys[i], b = keys[j];
-  if (a != b) return __clz(a ^ b);
-  return 32 + __clz((uint32_t)(i ^ j));
+  if (i == j) return 8 * (int)sizeof(K) + 32;
+  const K a = keys[i], b = keys[j];
+  if (a != b) return (sizeof(K) == 8) ? __clzll((long long)(a ^ b)) : __clz((unsigned)(a ^ b));
+  return 8 * (int)sizeof(K) + __clz((uint32_t)(i ^ j));
 }
 
-// tree_builder.cu:30-113 for internal node i of a tree over n keys.
-__device__ void karras_node(const uint32_t *keys, int n, int i, int *left, int *right,
+// tree_builder.cu:30-113 for internal node i of a tree over n keys.  The
+// stored prefix length is in the reference's 32-bit frame.
+template <typename K>
+__device__ void karras_node(const K *keys, int n, int i, int *left, int *right,
                             int *rfirst, int *rlast, int *plen, int *parent) {
   const int dright = lcp(keys, i, i + 1, n);
   const int dleft = lcp(keys, i, i - 1, n);
@@ -523,7 +597,7 @@ __device__ void karras_node(const uint32_t *keys, int n, int i, int *left, int *
   rfirst[i] = first;
   rlast[i] = last;
   const int node_prefix = lcp(keys, first, last, n);
-  plen[i] = node_prefix;
+  plen[i] = node_prefix - (8 * (int)sizeof(K) - 32);
   // findSplit (tree_builder.cu:64-84), including the candidate < last guard
   int split = first;
   if (first < last) {
@@ -556,7 +630,7 @@ __global__ void __launch_bounds__(kBlock) karras_kernel(Workspace ws) {
     ws.gcount[i] = ws.glast[i] - ws.gfirst[i] + 1;
     if (i == 0) ws.rparent[g == 1 ? 0 : g] = -1;
     if (i < g - 1)
-      karras_node(ws.uniq, g, i, ws.left, ws.right, ws.rfirst, ws.rlast, ws.plen, ws.rparent);
+      karras_node(ws.ukey, g, i, ws.left, ws.right, ws.rfirst, ws.rlast, ws.plen, ws.rparent);
   }
 }
 
@@ -571,9 +645,11 @@ __global__ void __launch_bounds__(kBlock)
 
 // -------------------------------------------------------------- plan ----
 
-// radix_to_octree.cu:124-138
-__device__ __forceinline__ int octree_level_of(int n_leaves, const int *plen, int r) {
-  const int prefix = (r < n_leaves) ? kSpatialBits : plen[r - n_leaves] - kPaddingBits;
+// radix_to_octree.cu:124-138.  Spatial prefix bits = prefix length in the
+// reference's 32-bit frame minus (32 - key bits); for a single system (30-bit
+// keys) that is the reference's plen - 2.
+__device__ __forceinline__ int octree_level_of(const Workspace &ws, int n_leaves, int r) {
+  const int prefix = (r < n_leaves) ? ws.key_bits : ws.plen[r - n_leaves] - (32 - ws.key_bits);
   return prefix / kDims;
 }
 
@@ -588,19 +664,19 @@ __device__ int plan_node(const Workspace &ws, int g, int r) {
     return 0;
   };
   if (r < g) {
-    if ((ws.uniq[r] & ~kSpatialMask) != 0u) return fail(1);
+    if ((ws.ukey[r] >> ws.key_bits) != 0ull) return fail(1);
   } else {
-    const int sp = ws.plen[r - g] - kPaddingBits;
-    if (sp < 0 || sp >= kSpatialBits) return fail(4);
+    const int sp = ws.plen[r - g] - (32 - ws.key_bits);
+    if (sp < 0 || sp >= ws.key_bits) return fail(4);
   }
   const int p = ws.rparent[r];
   int parent_level = 0;
   if (p != -1) {
     if (p < g || p >= nr) return fail(2);
-    parent_level = octree_level_of(g, ws.plen, p);
+    parent_level = octree_level_of(ws, g, p);
   }
-  const int node_level = (r < g) ? parent_level + 1 : octree_level_of(g, ws.plen, r);
-  if (node_level < 0 || node_level > kMaxLevel) return fail(3);
+  const int node_level = (r < g) ? parent_level + 1 : octree_level_of(ws, g, r);
+  if (node_level < 0 || node_level > ws.max_level) return fail(3);
   if (node_level < parent_level) return fail(3);
   ws.plevel[r] = node_level;
   ws.pcount[r] = node_level - parent_level;
@@ -617,7 +693,7 @@ __global__ void __launch_bounds__(kScanThreads) plan_kernel(Workspace ws) {
   const int g = sc->n_groups;
   if (g <= 0 || g > ws.n || sc->error) return;
   const int nr = 2 * g - 1;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[5], 1u);
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[kTilePlan], 1u);
   __syncthreads();
   const int tile = s_tile;
   const int base = tile * kScanTile;
@@ -663,7 +739,7 @@ __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
     c[1] = make_int4(-1, -1, -1, -1);
     ws.oparent[i] = -1;
     ws.olevel[i] = (i == 0) ? 0 : -1;
-    ws.oprefix[i] = 0u;
+    ws.oprefix[i] = 0ull;
     ws.ofirst[i] = -1;
     ws.ocount[i] = 0;
     ws.pending[i] = 0;
@@ -679,14 +755,14 @@ __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
   }
 }
 
-// octree_builder.cu:237-254
-__device__ __forceinline__ uint32_t prefix_at_level(uint32_t key, int level) {
-  if (level == 0) return 0u;
-  const int rem = kSpatialBits - level * kDims;
-  return key & (kSpatialMask & (~0u << rem));
+// octree_builder.cu:237-254 for keys of key_bits bits.
+__device__ __forceinline__ unsigned long long prefix_at_level(unsigned long long key, int level, int key_bits) {
+  if (level == 0) return 0ull;
+  const int rem = key_bits - level * kDims;
+  return (key >> rem) << rem;
 }
-__device__ __forceinline__ int octant_at_level(uint32_t key, int level) {
-  return (int)((key >> (kSpatialBits - level * kDims)) & 7u);
+__device__ __forceinline__ int octant_at_level(unsigned long long key, int level, int key_bits) {
+  return (int)((key >> (key_bits - level * kDims)) & 7ull);
 }
 
 // octree_builder.cu:275-412: each radix edge emits its chain of octree nodes
@@ -701,7 +777,7 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += gridDim.x * blockDim.x) {
     const int count = ws.pcount[r];
     const int node_level = ws.plevel[r];
-    if (count < 0 || node_level < 0 || node_level > kMaxLevel) {
+    if (count < 0 || node_level < 0 || node_level > ws.max_level) {
       record_error(sc, kStageOctree, 1);
       continue;
     }
@@ -714,16 +790,16 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
       record_error(sc, kStageOctree, 1);
       continue;
     }
-    uint32_t key;
+    unsigned long long key;
     if (r < g) {
-      key = ws.uniq[r];
+      key = ws.ukey[r];
     } else {
       const int f = ws.rfirst[r - g];
       if (f < 0 || f >= g) {
         record_error(sc, kStageOctree, 7);
         continue;
       }
-      key = ws.uniq[f];
+      key = ws.ukey[f];
     }
     int parent_node = 0;
     int anc = ws.rparent[r];
@@ -772,9 +848,9 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
       const int level = parent_level + local + 1;
       const int par = (local == 0) ? parent_node : node - 1;
       ws.olevel[node] = level;
-      ws.oprefix[node] = prefix_at_level(key, level);
+      ws.oprefix[node] = prefix_at_level(key, level, ws.key_bits);
       ws.oparent[node] = par;
-      const int prev = atomicCAS(&ws.children[(size_t)par * 8 + octant_at_level(key, level)], -1, node);
+      const int prev = atomicCAS(&ws.children[(size_t)par * 8 + octant_at_level(key, level, ws.key_bits)], -1, node);
       if (prev != -1 && prev != node) {
         record_error(sc, kStageOctree, 4);
         bad = true;
@@ -785,7 +861,7 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
     if (r < g) {
       const int leaf = first_node + count - 1;
       const int ll = parent_level + count;
-      if (ll <= 0 || ll > kMaxLevel) {
+      if (ll <= 0 || ll > ws.max_level) {
         record_error(sc, kStageOctree, 5);
         continue;
       }
@@ -805,28 +881,35 @@ __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int m = sc->n_nodes;
-  const double bx = sc->box[0], by = sc->box[1], bz = sc->box[2], bs = sc->box[3];
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
     const int level = ws.olevel[node];
-    if (level < 0 || level > kMaxLevel) {
+    if (level < 0 || level > ws.max_level) {
       record_error(sc, kStageGeometry, 1);
     } else {
-      const uint32_t prefix = ws.oprefix[node];
-      bool valid = (prefix & ~kSpatialMask) == 0u;
+      const unsigned long long prefix = ws.oprefix[node];
+      const int kb = ws.key_bits;
+      bool valid = (prefix >> kb) == 0ull;
       if (valid) {
         if (level == 0) {
-          valid = prefix == 0u;
+          valid = prefix == 0ull;
         } else {
-          const int rem = kSpatialBits - level * kDims;
-          valid = (prefix & ~(kSpatialMask & (~0u << rem))) == 0u;
+          const int rem = kb - level * kDims;
+          valid = (prefix & ((1ull << rem) - 1ull)) == 0ull;
         }
       }
       if (!valid) {
         record_error(sc, kStageGeometry, 2);
+      } else if (level < ws.sys_levels) {
+        // above the system roots of an ensemble: no cell, never visited
+        ws.cx[node] = 0.0;
+        ws.cy[node] = 0.0;
+        ws.cz[node] = 0.0;
+        ws.half[node] = 0.0;
       } else {
-        double cx = bx, cy = by, cz = bz, h = __dmul_rn(bs, 0.5);
-        for (int d = 1; d <= level; ++d) {
-          const int oct = (int)((prefix >> (kSpatialBits - d * kDims)) & 7u);
+        const double *box = ws.sys_box + 4 * (size_t)(prefix >> kSpatialBits);
+        double cx = box[0], cy = box[1], cz = box[2], h = __dmul_rn(box[3], 0.5);
+        for (int d = ws.sys_levels + 1; d <= level; ++d) {
+          const int oct = (int)((prefix >> (kb - d * kDims)) & 7ull);
           const double ch = __dmul_rn(h, 0.5);
           cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
           cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
@@ -904,7 +987,7 @@ __global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
     int parent = ws.oparent[done];
     int climbs = 0;
     while (parent != -1) {
-      if (parent < 0 || parent >= m || ++climbs > kMaxLevel + 1) {
+      if (parent < 0 || parent >= m || ++climbs > ws.max_level + 1) {
         record_error(sc, kStagePhysics, 5);
         break;
       }
@@ -992,7 +1075,7 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
     while (v != 0) {
       pre += ws.preoff[v];
       v = ws.oparent[v];
-      if (v < 0 || ++guard > kMaxLevel + 1) {
+      if (v < 0 || ++guard > ws.max_level + 1) {
         record_error(sc, kStageLayout, 1);
         break;
       }
@@ -1003,7 +1086,9 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
       continue;
     }
     const double h = ws.half[node];
-    if (!(h > 0.0)) record_error(sc, kStageTraversal, 8);
+    const int lvl = ws.olevel[node];
+    if (lvl == ws.sys_levels) ws.root_pre[ws.oprefix[node] >> kSpatialBits] = pre;
+    if (!(h > 0.0) && lvl >= ws.sys_levels) record_error(sc, kStageTraversal, 8);
     int pc = ws.ocount[node];
     const int cnt = ws.child_count[node];
     const int f = ws.ofirst[node];
@@ -1058,7 +1143,8 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
     const int gmax = ws.group_max;
     const int np = ws.psub[node];
     if (np <= gmax) {
-      if (node == 0 && np > 0) ws.tflag[0] = 1;  // the whole system is one group
+      // a whole system smaller than a group is one group
+      if (ws.olevel[node] == ws.sys_levels && np > 0) ws.tflag[ws.pfirst[node]] = 1;
       continue;
     }
     if (ws.ocount[node] > 0) {
@@ -1069,11 +1155,13 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
         if (f + k >= 0 && f + k < ws.n) ws.tflag[f + k] = 1;
       continue;
     }
+    const bool virt = ws.olevel[node] < ws.sys_levels;  // children are other systems
     int run = 0;
     for (int o = 0; o < 8; ++o) {
       const int c = ws.children[(size_t)node * 8 + o];
       if (c <= 0 || c >= m) continue;
       const int cp = ws.psub[c];
+      if (virt) run = 0;
       if (cp > gmax) {
         run = 0;
         continue;
@@ -1096,7 +1184,7 @@ __global__ void __launch_bounds__(kScanThreads) group_scan_kernel(Workspace ws) 
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int n = ws.n;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[6], 1u);
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[kTileTargetGroups], 1u);
   __syncthreads();
   const int tile = s_tile;
   const int base = tile * kScanTile;
@@ -1132,20 +1220,27 @@ __global__ void retarget_reset_kernel(DevScalars *sc) {
   if (threadIdx.x == 0) {
     sc->work_counter = 0;
     sc->n_tgroups = 0;
-    sc->tile_counter[6] = 0;
+    sc->tile_counter[kTileTargetGroups] = 0;
     sc->interactions = 0;
     sc->mac_tests = 0;
     sc->stack_overflow = 0;
   }
 }
 
+// Self-test of the bounded waits: one warp looks back from tile 1 while tile
+// 0 never publishes; the spin limit must end the wait and record the
+// timeout code instead of hanging.
+__global__ void lookback_probe_kernel(unsigned long long *status, DevScalars *sc) {
+  if (threadIdx.x < 32) (void)warp_lookback(status, 1, 1ull, sc, kStageGroups);
+}
+
 // Sorted packed pairs -> caller key / index arrays (sort-only entry point).
-__global__ void __launch_bounds__(kBlock) split_pairs_kernel(const unsigned long long *pairs, int n,
+__global__ void __launch_bounds__(kBlock) split_pairs_kernel(const unsigned long long *pairs, int n, int shift,
                                                              uint32_t *keys, uint32_t *idx) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const unsigned long long pr = pairs[i];
-    keys[i] = (uint32_t)(pr >> 32);
-    idx[i] = (uint32_t)(pr & 0xffffffffu);
+    keys[i] = (uint32_t)(pr >> shift);
+    idx[i] = (uint32_t)(pr & ((1ull << shift) - 1ull));
   }
 }
 
@@ -1153,7 +1248,7 @@ __global__ void __launch_bounds__(kBlock) split_pairs_kernel(const unsigned long
 // topology entry points.
 __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x)
-    ws.pairs_a[i] = ((unsigned long long)keys[i] << 32) | (unsigned)i;
+    ws.pairs_a[i] = ((unsigned long long)keys[i] << ws.pack_shift) | (unsigned)i;
 }
 
 }  // namespace
@@ -1162,10 +1257,11 @@ __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const u
 
 cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s) {
   reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
-  count_launches(1);
-  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kSortPasses * 256, s);
+  reset_sys_kernel<<<(6 * ws.n_systems + 255) / 256, 256, 0, s>>>(ws.sys_bb, ws.n_systems);
+  count_launches(2);
+  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kMaxSortPasses * 256, s);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)kSortPasses * ws.sort_tiles * 256, s);
+  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)ws.sort_passes * ws.sort_tiles * 256, s);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(ws.scan_status, 0,
                       sizeof(unsigned long long) * (size_t)(2 * ws.scan_tiles_n + ws.scan_tiles_r), s);
@@ -1194,15 +1290,16 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s) {
   if (blocks < 1) blocks = 1;
   encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
   unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
-  for (int p = 0; p < kSortPasses; ++p) {
+  for (int p = 0; p < ws.sort_passes; ++p) {
     onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
-        src, dst, ws.n, p, ws.digit_hist, ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
+        src, dst, ws.n, p, ws.pack_shift + 8 * p, ws.digit_hist,
+        ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
     unsigned long long *t = src;
     src = dst;
     dst = t;
   }
-  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, 1);
-  count_launches(2 + kSortPasses);
+  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, src, 1);
+  count_launches(2 + ws.sort_passes);
   return cudaGetLastError();
 }
 
@@ -1223,9 +1320,10 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
 
 cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s) {
   reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
-  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kSortPasses * 256, s);
+  reset_sys_kernel<<<1, 32, 0, s>>>(ws.sys_bb, ws.n_systems);
+  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kMaxSortPasses * 256, s);
   if (e != cudaSuccess) return e;
-  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)kSortPasses * ws.sort_tiles * 256, s);
+  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)ws.sort_passes * ws.sort_tiles * 256, s);
   if (e != cudaSuccess) return e;
   int blocks = (ws.n + kBlock - 1) / kBlock;
   const int cap = grid_for(ws, 4);
@@ -1234,15 +1332,22 @@ cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx
   kd_bbox_kernel<<<blocks, kBlock, 0, s>>>(ws, 0.0, 0);
   encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
   unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
-  for (int p = 0; p < kSortPasses; ++p) {
+  for (int p = 0; p < ws.sort_passes; ++p) {
     onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
-        src, dst, ws.n, p, ws.digit_hist, ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
+        src, dst, ws.n, p, ws.pack_shift + 8 * p, ws.digit_hist,
+        ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
     unsigned long long *t = src;
     src = dst;
     dst = t;
   }
-  split_pairs_kernel<<<blocks, kBlock, 0, s>>>(src, ws.n, keys, idx);
-  count_launches(4 + kSortPasses);
+  split_pairs_kernel<<<blocks, kBlock, 0, s>>>(src, ws.n, ws.pack_shift, keys, idx);
+  count_launches(4 + ws.sort_passes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lookback_probe(unsigned long long *status, DevScalars *sc, cudaStream_t s) {
+  lookback_probe_kernel<<<1, 32, 0, s>>>(status, sc);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -1262,7 +1367,7 @@ cudaError_t launch_retarget(Workspace &ws, cudaStream_t s) {
 
 cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys, cudaStream_t s) {
   pack_keys_kernel<<<grid_for(ws, 4), kBlock, 0, s>>>(ws, sorted_keys);
-  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, 0);
+  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, ws.pairs_a, 0);
   count_launches(2);
   return cudaGetLastError();
 }

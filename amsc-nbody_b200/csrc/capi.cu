@@ -8,6 +8,7 @@
 #include "nbb.h"
 #include "nbb_internal.cuh"
 
+#include <algorithm>
 #include <atomic>
 #include <climits>
 #include <cmath>
@@ -61,7 +62,14 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 // Messages of the reference's device error codes, by stage.
 const char *device_message(int stage, int code) {
-  if (code == kCodeTimeout) return "A bounded device-side wait gave up (look-back predecessor never published)";
+  if (code == kCodeTimeout) {
+    switch (stage) {
+      case kStageSort: return "A bounded device-side wait gave up in the radix sort look-back";
+      case kStageGroups: return "A bounded device-side wait gave up in a leaf/target group scan look-back";
+      case kStagePlan: return "A bounded device-side wait gave up in the radix-to-octree plan scan look-back";
+      default: return "A bounded device-side wait gave up";
+    }
+  }
   switch (stage) {
     case kStageBbox:
       return code == 1 ? "Particle positions must be finite to compute a bounding box."
@@ -129,11 +137,11 @@ int device_status(int word) {
 }
 
 // Octree node capacity: every level L holds at most min(8^L, G) nodes and
-// G <= n, over levels 0..10.
-int node_capacity(int n) {
+// G <= n, over levels 0..max_level.
+int node_capacity(int n, int max_level) {
   long long cap = 1;
   long long width = 1;
-  for (int level = 0; level <= kMaxLevel; ++level) {
+  for (int level = 0; level <= max_level; ++level) {
     cap += (width < n) ? width : n;
     if (width < (1ll << 40)) width *= 8;
   }
@@ -158,10 +166,17 @@ struct Allocation {
 
 // Allocate every buffer of a workspace for n particles (state included when
 // with_state).  All device memory is taken here; nothing is allocated later.
-cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_state) {
+cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_state, int n_systems = 1) {
   ws = Workspace{};
   ws.n = n;
-  ws.cap_nodes = node_capacity(n);
+  ws.n_systems = n_systems;
+  ws.sys_levels = 0;
+  while ((1 << (3 * ws.sys_levels)) < n_systems) ++ws.sys_levels;
+  ws.key_bits = kSpatialBits + kDims * ws.sys_levels;
+  ws.max_level = ws.key_bits / kDims;
+  ws.pack_shift = 64 - ws.key_bits;
+  ws.sort_passes = (ws.key_bits + 7) / 8;
+  ws.cap_nodes = node_capacity(n, ws.max_level);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&ws.num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -175,16 +190,22 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
     GET(ws.ax, N); GET(ws.ay, N); GET(ws.az, N);
     GET(ws.type, N);
   }
+  const size_t S = (size_t)n_systems;
+  if (n_systems > 1) {
+    GET(ws.sys_of, N);
+    GET(ws.sys_eps, S);
+  }
   GET(ws.sc, 1);
+  GET(ws.sys_bb, 6 * S); GET(ws.sys_box, 4 * S); GET(ws.root_pre, S);
   GET(ws.pairs_a, N); GET(ws.pairs_b, N);
-  GET(ws.digit_hist, (size_t)kSortPasses * 256);
+  GET(ws.digit_hist, (size_t)kMaxSortPasses * 256);
   ws.sort_tiles = (n + kSortTile - 1) / kSortTile;
-  GET(ws.sort_status, (size_t)kSortPasses * ws.sort_tiles * 256);
+  GET(ws.sort_status, (size_t)ws.sort_passes * ws.sort_tiles * 256);
   ws.scan_tiles_n = (n + kScanTile - 1) / kScanTile;
   ws.scan_tiles_r = (2 * n - 1 + kScanTile - 1) / kScanTile;
   GET(ws.scan_status, (size_t)(2 * ws.scan_tiles_n + ws.scan_tiles_r));
-  GET(ws.keys, N); GET(ws.idx, N); GET(ws.pm4, N);
-  GET(ws.uniq, N); GET(ws.gfirst, N); GET(ws.gcount, N); GET(ws.glast, N);
+  GET(ws.keys, N); GET(ws.idx, N); GET(ws.pm4, N); GET(ws.psys, N);
+  GET(ws.ukey, N); GET(ws.uniq, N); GET(ws.gfirst, N); GET(ws.gcount, N); GET(ws.glast, N);
   GET(ws.left, N); GET(ws.right, N); GET(ws.rfirst, N); GET(ws.rlast, N); GET(ws.plen, N);
   GET(ws.rparent, 2 * N);
   GET(ws.plevel, 2 * N); GET(ws.pcount, 2 * N); GET(ws.poffset, 2 * N);
@@ -199,6 +220,8 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.node_kids, 8 * C);
 #undef GET
   e = cudaMemset(ws.sc, 0, sizeof(DevScalars));
+  if (e != cudaSuccess) return e;
+  e = cudaMemset(ws.root_pre, 0, S * sizeof(int));
   if (e != cudaSuccess) return e;
   return configure_traversal(ws);
 }
@@ -228,6 +251,9 @@ int export_workspace(const Workspace &ws, nbb_tree_export *o, cudaStream_t s, bo
   if (m > o->m_capacity && (o->children || o->oparent || o->olevel || o->oprefix || o->ofirst ||
                             o->ocount || o->child_count || o->cx || o->mass))
     return fail(NBB_ERR_INVALID_ARGUMENT, "export m_capacity is smaller than the octree node count");
+  if (ws.key_bits > 32 && (o->keys || o->uniq || o->oprefix))
+    return fail(NBB_ERR_INVALID_ARGUMENT,
+                "keys of an ensemble with more than 4 systems exceed 32 bits; pass null keys, uniq and oprefix");
   const size_t G = (size_t)g, R = g > 0 ? (size_t)(2 * g - 1) : 0, I = g > 1 ? (size_t)(g - 1) : 0;
   const size_t M = (size_t)m;
   NBB_CUDA(d2h_opt(o->keys, ws.keys, (size_t)n, s), "export keys");
@@ -247,7 +273,13 @@ int export_workspace(const Workspace &ws, nbb_tree_export *o, cudaStream_t s, bo
   NBB_CUDA(d2h_opt(o->children, ws.children, 8 * M, s), "export octree");
   NBB_CUDA(d2h_opt(o->oparent, ws.oparent, M, s), "export octree");
   NBB_CUDA(d2h_opt(o->olevel, ws.olevel, M, s), "export octree");
-  NBB_CUDA(d2h_opt(o->oprefix, ws.oprefix, M, s), "export octree");
+  if (o->oprefix && M) {
+    std::vector<unsigned long long> wide(M);
+    NBB_CUDA(cudaMemcpyAsync(wide.data(), ws.oprefix, M * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+             "export octree");
+    NBB_CUDA(cudaStreamSynchronize(s), "export synchronisation");
+    for (size_t k = 0; k < M; ++k) o->oprefix[k] = (uint32_t)wide[k];
+  }
   NBB_CUDA(d2h_opt(o->ofirst, ws.ofirst, M, s), "export octree");
   NBB_CUDA(d2h_opt(o->ocount, ws.ocount, M, s), "export octree");
   if (particles) {
@@ -319,6 +351,7 @@ struct nbb_sim {
   cudaGraph_t step_graph_def = nullptr;
   uint64_t graph_kernels = 0;
   int tuned_group_size = 0;
+  double min_softening = 0.0;  // ensembles: smallest per-system softening
 };
 
 extern "C" {
@@ -333,6 +366,26 @@ void nbb_config_default(nbb_config *cfg) {
   cfg->group_size = 0;
   cfg->use_graph = 1;
   cfg->device = 0;
+}
+
+int nbb_selftest_bounded_wait(void) {
+  Allocation al;
+  cudaStream_t s = nullptr;
+  NBB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  DevScalars *sc = nullptr;
+  unsigned long long *status = nullptr;
+  cudaError_t e = al.get(sc, 1);
+  if (e == cudaSuccess) e = al.get(status, 2);
+  if (e == cudaSuccess) e = cudaMemsetAsync(sc, 0, sizeof(DevScalars), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(status, 0, 2 * sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = launch_lookback_probe(status, sc, s);
+  int word = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&word, &sc->error, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return cuda_fail(e, "bounded-wait self-test");
+  if (word == 0) return fail(NBB_ERR_DEVICE, "bounded-wait self-test: the wait did not report a timeout");
+  return device_status(word);
 }
 
 int nbb_measure_fma_tflops(int precision, double *tflops) {
@@ -362,9 +415,10 @@ static int validate_config(const nbb_config *c) {
   return NBB_OK;
 }
 
-int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const double *x,
-                   const double *y, const double *z, const double *vx, const double *vy,
-                   const double *vz, const uint8_t *type, int on_device, nbb_sim **out) {
+static int create_sim(const nbb_config *cfg, size_t n, int n_systems, const int64_t *offsets,
+                      const double *softening, const double *mass, const double *x, const double *y,
+                      const double *z, const double *vx, const double *vy, const double *vz,
+                      const uint8_t *type, int on_device, nbb_sim **out) {
   if (!cfg || !out) return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_sim_create: null argument");
   *out = nullptr;
   int st = validate_config(cfg);
@@ -374,12 +428,37 @@ int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const do
     return fail(NBB_ERR_OVERFLOW, "Particle count exceeds the tree representation");
   if (!mass || !x || !y || !z || !vx || !vy || !vz)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Particle arrays must not be null");
+  std::vector<int> sys_of;
+  std::vector<double> eps;
+  double min_eps = cfg->softening;
+  if (n_systems > 1) {
+    if (n_systems > kMaxSystems)
+      return fail(NBB_ERR_INVALID_ARGUMENT, "An ensemble holds at most " + std::to_string(kMaxSystems) + " systems");
+    if (!offsets || offsets[0] != 0 || offsets[n_systems] != (int64_t)n)
+      return fail(NBB_ERR_INVALID_ARGUMENT, "Ensemble offsets must start at 0 and end at the particle count");
+    const int key_bits = kSpatialBits + kDims * 3;
+    if ((unsigned long long)n >= (1ull << (64 - key_bits)))
+      return fail(NBB_ERR_OVERFLOW, "Ensemble particle count exceeds the sort key layout");
+    sys_of.resize(n);
+    eps.resize((size_t)n_systems);
+    min_eps = INFINITY;
+    for (int k = 0; k < n_systems; ++k) {
+      if (offsets[k + 1] <= offsets[k])
+        return fail(NBB_ERR_INVALID_ARGUMENT, "Every ensemble system needs at least one particle");
+      eps[k] = softening ? softening[k] : cfg->softening;
+      if (!finite_nonneg(eps[k]))
+        return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation softening must be finite and non-negative");
+      min_eps = std::min(min_eps, eps[k]);
+      for (int64_t i = offsets[k]; i < offsets[k + 1]; ++i) sys_of[(size_t)i] = k;
+    }
+  }
   NBB_CUDA(cudaSetDevice(cfg->device), "cudaSetDevice");
   nbb_sim *sim = new (std::nothrow) nbb_sim();
   if (!sim) return fail(NBB_ERR_CUDA, "host allocation failed");
   sim->cfg = *cfg;
+  sim->min_softening = min_eps;
   cudaError_t e = cudaStreamCreateWithFlags(&sim->own_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = alloc_workspace(sim->ws, sim->alloc, (int)n, true);
+  if (e == cudaSuccess) e = alloc_workspace(sim->ws, sim->alloc, (int)n, true, n_systems > 1 ? n_systems : 1);
   if (e != cudaSuccess) {
     if (sim->own_stream) cudaStreamDestroy(sim->own_stream);
     delete sim;
@@ -397,6 +476,11 @@ int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const do
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.ax, 0, bytes, sim->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.ay, 0, bytes, sim->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(ws.az, 0, bytes, sim->stream);
+  if (e == cudaSuccess && n_systems > 1) {
+    e = cudaMemcpyAsync(ws.sys_of, sys_of.data(), n * sizeof(int), cudaMemcpyHostToDevice, sim->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ws.sys_eps, eps.data(), eps.size() * sizeof(double), cudaMemcpyHostToDevice, sim->stream);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(sim->stream);
   if (e != cudaSuccess) {
     nbb_sim_destroy(sim);
@@ -404,6 +488,26 @@ int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const do
   }
   *out = sim;
   return ok();
+}
+
+int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass, const double *x,
+                   const double *y, const double *z, const double *vx, const double *vy,
+                   const double *vz, const uint8_t *type, int on_device, nbb_sim **out) {
+  return create_sim(cfg, n, 1, nullptr, nullptr, mass, x, y, z, vx, vy, vz, type, on_device, out);
+}
+
+int nbb_ensemble_create(const nbb_config *cfg, int n_systems, const int64_t *offsets,
+                        const double *softening, const double *mass, const double *x, const double *y,
+                        const double *z, const double *vx, const double *vy, const double *vz,
+                        int on_device, nbb_sim **out) {
+  if (n_systems <= 0 || !offsets) return fail(NBB_ERR_INVALID_ARGUMENT, "An ensemble needs at least one system");
+  const size_t n = (size_t)offsets[n_systems];
+  if (n_systems == 1) {
+    nbb_config c = *cfg;
+    if (softening) c.softening = softening[0];
+    return create_sim(&c, n, 1, nullptr, nullptr, mass, x, y, z, vx, vy, vz, nullptr, on_device, out);
+  }
+  return create_sim(cfg, n, n_systems, offsets, softening, mass, x, y, z, vx, vy, vz, nullptr, on_device, out);
 }
 
 static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
@@ -417,6 +521,10 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size
                                           : (sim->tuned_group_size > 0 ? sim->tuned_group_size : 32);
   tp.group_mode = default_group_mode(tp.precision);
+  if (sim->ws.n_systems > 1) {
+    tp.group_mode = 1;  // a warp's targets must share a system
+    tp.soft = sim->min_softening;
+  }
   return tp;
 }
 
@@ -903,6 +1011,7 @@ int nbb_octree_from_keys(const uint32_t *sorted_keys, int n, nbb_tree_export *ou
   Scratch sc;
   NBB_CUDA(cudaStreamCreateWithFlags(&sc.s, cudaStreamNonBlocking), "create stream");
   NBB_CUDA(alloc_workspace(sc.ws, sc.al, n, false), "allocate workspace");
+  sc.ws.pack_shift = 32;  // caller keys may use all 32 bits (rejected by the plan)
   uint32_t *dk = nullptr;
   NBB_CUDA(sc.al.get(dk, (size_t)n), "allocate keys");
   NBB_CUDA(cudaMemcpyAsync(dk, sorted_keys, (size_t)n * 4, cudaMemcpyHostToDevice, sc.s), "copy keys");

@@ -43,7 +43,7 @@ struct DevScalars {
   int error;                     // sticky first error (not reset per step)
   unsigned int ticket_bbox;
   unsigned int ticket_encode;
-  unsigned int tile_counter[8];  // dynamic tile ids of single-pass kernels
+  unsigned int tile_counter[8];  // dynamic tile ids: sort passes, then scans
   unsigned int work_counter;     // traversal work queue
   int n_tgroups;                 // traversal target groups
   unsigned int stack_overflow;   // mixed traversal nodes accepted on overflow
@@ -55,10 +55,19 @@ struct DevScalars {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs
-constexpr int kSortPasses = 4;                        // 8-bit digits, bits 32..63
+constexpr int kSortPasses = 4;     // 8-bit digits over a single system's 30-bit keys
+constexpr int kMaxSortPasses = 5;  // ensemble keys: up to 9 system bits + 30 Morton bits
 
 // Largest target group supported (two targets per lane of a warp).
 constexpr int kGroupMaxLimit = 64;
+// Largest ensemble: 3 octree levels of system id.
+constexpr int kMaxSystems = 512;
+
+// Dynamic tile-id counters (DevScalars::tile_counter): one per sort pass,
+// then one per single-pass scan kernel.
+constexpr int kTileGroups = kMaxSortPasses;      // 5
+constexpr int kTilePlan = kMaxSortPasses + 1;    // 6
+constexpr int kTileTargetGroups = kMaxSortPasses + 2;  // 7
 
 // Single-pass scan tiling.
 constexpr int kScanThreads = 256;
@@ -74,13 +83,27 @@ struct Workspace {
   int mixed_grid[2][2] = {{0, 0}, {0, 0}};  // [track source][targets per lane - 1]
   int group_max = 32;   // largest octree target group (32 x targets per lane)
 
+  // key layout: an ensemble's system id sits above the 30 Morton bits and
+  // adds sys_levels octree levels above the system roots
+  int n_systems = 1;
+  int sys_levels = 0;    // ceil(log8(n_systems)), at most 3
+  int key_bits = 30;     // 30 + 3 * sys_levels
+  int max_level = 10;    // key_bits / 3
+  int pack_shift = 34;   // sort pairs: key << pack_shift | particle index
+  int sort_passes = 4;   // ceil(key_bits / 8)
+
   // particle state, original order (SoA, FP64)
   double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
   double *vx = nullptr, *vy = nullptr, *vz = nullptr;
   double *ax = nullptr, *ay = nullptr, *az = nullptr;
   uint8_t *type = nullptr;
+  int *sys_of = nullptr;       // ensemble: system of each particle (original order)
 
   DevScalars *sc = nullptr;
+  unsigned long long *sys_bb = nullptr;  // 6 per system: encoded min xyz, max xyz
+  double *sys_box = nullptr;             // 4 per system: centre xyz, side
+  double *sys_eps = nullptr;             // ensemble: softening per system
+  int *root_pre = nullptr;               // preorder index of each system's root
 
   // sort
   unsigned long long *pairs_a = nullptr, *pairs_b = nullptr;  // n each
@@ -91,12 +114,15 @@ struct Workspace {
   int scan_tiles_n = 0;   // tiles over n
   int scan_tiles_r = 0;   // tiles over 2n-1
 
-  // Morton keys / permutation (reference MortonKeys layout)
+  // Morton keys / permutation (reference MortonKeys layout; keys hold the low
+  // 32 bits of the full key)
   uint32_t *keys = nullptr, *idx = nullptr;
+  int *psys = nullptr;     // system of each sorted particle
   double4 *pm4 = nullptr;  // Morton-ordered particles {x, y, z, m}
 
   // leaf groups (MortonLeafGroups)
-  uint32_t *uniq = nullptr;
+  unsigned long long *ukey = nullptr;  // full unique keys
+  uint32_t *uniq = nullptr;            // their low 32 bits (reference layout)
   int *gfirst = nullptr, *gcount = nullptr, *glast = nullptr;
 
   // radix tree (Tree): internal n-1, all nodes 2n-1
@@ -108,7 +134,7 @@ struct Workspace {
 
   // octree, reference numbering (Octree), cap_nodes
   int *children = nullptr, *oparent = nullptr, *olevel = nullptr;
-  uint32_t *oprefix = nullptr;
+  unsigned long long *oprefix = nullptr;
   int *ofirst = nullptr, *ocount = nullptr, *child_count = nullptr,
       *pending = nullptr;
   double *cx = nullptr, *cy = nullptr, *cz = nullptr, *half = nullptr;
@@ -210,6 +236,8 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s);
 // Rebuild the octree target groups for ws.group_max on the current tree and
 // reset the traversal counters (used by the group-size autotuner).
 cudaError_t launch_retarget(Workspace &ws, cudaStream_t s);
+// Bounded-wait self-test: a look-back whose predecessor never publishes.
+cudaError_t launch_lookback_probe(unsigned long long *status, DevScalars *sc, cudaStream_t s);
 // Traversal (+ optional fused second half kick).
 cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p,
                              cudaStream_t s);

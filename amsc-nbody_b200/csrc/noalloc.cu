@@ -29,8 +29,10 @@ constexpr size_t round_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kMaxN = NBB_NOALLOC_MAX_PARTICLES;
 constexpr size_t kMaxTiles = (kMaxN + kSortTile - 1) / kSortTile;
 constexpr size_t kOffScalars = 0;
-constexpr size_t kOffHist = round_up(kOffScalars + sizeof(DevScalars));
-constexpr size_t kOffStatus = round_up(kOffHist + sizeof(uint32_t) * kSortPasses * 256);
+constexpr size_t kOffSysBB = round_up(kOffScalars + sizeof(DevScalars));
+constexpr size_t kOffSysBox = round_up(kOffSysBB + 6 * sizeof(unsigned long long));
+constexpr size_t kOffHist = round_up(kOffSysBox + 4 * sizeof(double));
+constexpr size_t kOffStatus = round_up(kOffHist + sizeof(uint32_t) * nbb::kMaxSortPasses * 256);
 constexpr size_t kOffPairsA = round_up(kOffStatus + sizeof(uint32_t) * kSortPasses * kMaxTiles * 256);
 constexpr size_t kOffPairsB = round_up(kOffPairsA + sizeof(unsigned long long) * kMaxN);
 constexpr size_t kScratchBytes = round_up(kOffPairsB + sizeof(unsigned long long) * kMaxN);
@@ -88,6 +90,8 @@ int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z, s
   ws.y = const_cast<double *>(y);
   ws.z = const_cast<double *>(z);
   ws.sc = reinterpret_cast<DevScalars *>(base + kOffScalars);
+  ws.sys_bb = reinterpret_cast<unsigned long long *>(base + kOffSysBB);
+  ws.sys_box = reinterpret_cast<double *>(base + kOffSysBox);
   ws.digit_hist = reinterpret_cast<uint32_t *>(base + kOffHist);
   ws.sort_tiles = (int)((n + kSortTile - 1) / kSortTile);
   ws.sort_status = reinterpret_cast<uint32_t *>(base + kOffStatus);

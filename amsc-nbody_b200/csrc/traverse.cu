@@ -63,7 +63,6 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
   const int n = ws.n;
   const int m = sc->n_nodes;
   const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
-  const double soft2 = __dmul_rn(p.soft, p.soft);
   const double g = p.g;
   long long inter = 0, tests = 0;
   bool singular = false;
@@ -78,10 +77,16 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
     const bool valid = s < g1 && s < n;
     double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
     if (valid) t = ws.pm4[s];
+    // a warp's targets belong to one system: walk that system's subtree
+    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+    const int root = ws.root_pre[sys];
+    const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
+    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+    const double soft2 = __dmul_rn(soft, soft);
     double ax = 0.0, ay = 0.0, az = 0.0;
-    int resume = valid ? 0 : INT_MAX;
+    int resume = valid ? root : INT_MAX;
     int node = __reduce_min_sync(kFull, resume);
-    while (node < m) {
+    while (node < end) {
       // every record of the node in one round trip (warp-uniform address:
       // one broadcast transaction each)
       const int4 meta = ws.node_meta[node];
@@ -287,7 +292,6 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
   const int n = ws.n;
   const int m = sc->n_nodes;
   const int n_groups = p.group_mode ? sc->n_tgroups : (n + 32 * kTPL - 1) / (32 * kTPL);
-  const float eps2 = (float)(p.soft * p.soft);
   const unsigned lt = lanemask_lt();
   long long tests = 0;
   unsigned overflow = 0;
@@ -335,9 +339,14 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
       T.ty[q] = (float)(tp[q].y - gcy);
       T.tz[q] = (float)(tp[q].z - gcz);
     }
+    // a group's targets belong to one system: walk that system's subtree
+    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+    const int root = ws.root_pre[sys];
+    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+    const float eps2 = (float)(soft * soft);
     int ls = 0;
-    if (lane == 0) stack[0] = 0;
-    int sp = (m > 0) ? 1 : 0;
+    if (lane == 0) stack[0] = root;
+    int sp = (m > 0 && root >= 0 && root < m) ? 1 : 0;
     __syncwarp();
     while (sp > 0) {
       int k = sp < 32 ? sp : 32;

@@ -8,7 +8,7 @@ marshals arguments.
 """
 from ._lib import (PRECISION_FP64, PRECISION_MIXED, DeviceError, DomainError, InvalidArgument,
                    LogicError, NbbError, NoDevice, OverflowErrorNbb, load)
-from .api import (G_SI, BarnesHutParameters, Simulation, SimulationConfig, compute_accelerations,
+from .api import (G_SI, BarnesHutParameters, EnsembleSimulation, Simulation, SimulationConfig, compute_accelerations,
                   compute_direct_accelerations, computeBarnesHutAcceleration, kernel_launch_count,
                   measure_fma_tflops,
                   leapfrog_kick, leapfrog_kick_drift, node_capacity, octree_from_keys, radix_tree)
@@ -17,7 +17,7 @@ from .ics import ParticleData
 __all__ = [
     "PRECISION_FP64", "PRECISION_MIXED", "DeviceError", "DomainError", "InvalidArgument",
     "LogicError", "NbbError", "NoDevice", "OverflowErrorNbb", "load", "G_SI",
-    "BarnesHutParameters", "Simulation", "SimulationConfig", "compute_accelerations",
+    "BarnesHutParameters", "EnsembleSimulation", "Simulation", "SimulationConfig", "compute_accelerations",
     "compute_direct_accelerations", "computeBarnesHutAcceleration", "kernel_launch_count",
     "measure_fma_tflops",
     "leapfrog_kick", "leapfrog_kick_drift", "node_capacity", "octree_from_keys", "radix_tree",

@@ -66,6 +66,7 @@ class OctreeView(C.Structure):
 SIGNATURES = {
     "nbb_config_default": (None, [_P]),
     "nbb_sim_create": (_I, [_P, _Z] + [_P] * 8 + [_I, _P]),
+    "nbb_ensemble_create": (_I, [_P, _I, _P, _P] + [_P] * 7 + [_I, _P]),
     "nbb_sim_initialize": (_I, [_P]),
     "nbb_sim_step": (_I, [_P]),
     "nbb_sim_run": (_I, [_P, C.c_uint64]),
@@ -89,6 +90,7 @@ SIGNATURES = {
     "nbb_octree_from_keys": (_I, [_P, _I, _P]),
     "nbb_radix_tree": (_I, [_P, _I] + [_P] * 6),
     "nbb_measure_fma_tflops": (_I, [_I, _P]),
+    "nbb_selftest_bounded_wait": (_I, []),
     "nbb_last_error_message": (C.c_char_p, []),
     "nbb_last_error_code": (_I, []),
     "nbb_kernel_launch_count": (C.c_uint64, []),

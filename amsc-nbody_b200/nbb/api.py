@@ -152,6 +152,32 @@ class Simulation:
         return _export(lambda e: self._lib.nbb_sim_export(self._handle, C.byref(e)), self._n, m_capacity)
 
 
+class EnsembleSimulation(Simulation):
+    """Independent systems advanced together, one launch per stage
+    (nbb_ensemble_create): system k owns particles
+    [offsets[k], offsets[k+1]) and has its own softening.  Every Simulation
+    method applies; state arrays cover all systems back to back."""
+
+    def __init__(self, ensemble, config: SimulationConfig):
+        lib = _lib.load()
+        self._lib = lib
+        self._handle = C.c_void_p()
+        p = ensemble.particles
+        self._n = len(p)
+        arrs = [_f64(a) for a in p.arrays()]
+        offsets = np.ascontiguousarray(ensemble.offsets, dtype=np.int64)
+        if offsets.ndim != 1 or offsets.size < 2 or int(offsets[-1]) != self._n:
+            raise _lib.InvalidArgument(_lib.ERR_INVALID_ARGUMENT,
+                                       "ensemble offsets must end at the particle count "
+                                       f"({self._n}), got {offsets[-1] if offsets.size else None}")
+        eps = None if ensemble.softening is None else _f64(ensemble.softening)
+        cfg = config.to_c()
+        check(lib.nbb_ensemble_create(C.byref(cfg), int(offsets.size - 1), ptr(offsets), ptr(eps),
+                                      *[ptr(a) for a in arrs], 0, C.byref(self._handle)))
+        self.config = config
+        self.offsets = offsets
+
+
 _EXPORT_FIELDS = [
     ("keys", np.uint32, "n"), ("idx", np.uint32, "n"), ("uniq", np.uint32, "n"),
     ("gfirst", np.int32, "n"), ("gcount", np.int32, "n"), ("left", np.int32, "n"),

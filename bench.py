@@ -288,8 +288,8 @@ class _Null:
 
 
 # Algorithmic bytes of the rebuild (the minimum each stage must move), per
-# particle, per unique-key group, per radix node and per octree node; the
-# derivation is tabulated in DESIGN.md.
+# particle, per unique-key group, per radix node and per octree node: each
+# term is the sum of the arrays that stage must read once and write once.
 BUILD_BYTES_PER_PARTICLE = 120 + 32 + 64 + 80 + 32  # KD+bbox, encode, 4 sort passes, groups+gather, leaf mass
 BUILD_BYTES_PER_GROUP = 12 + 28                     # group arrays, Karras internal node
 BUILD_BYTES_PER_RADIX_NODE = 20 + 40                # plan + scan, materialise

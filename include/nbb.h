@@ -79,6 +79,19 @@ int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass,
                    const double *vx, const double *vy, const double *vz,
                    const uint8_t *type, int on_device, nbb_sim **out);
 
+/* No counterpart in the reference (it steps one system per Simulation):
+ * n_systems independent systems stored back to back -- system k owns
+ * particles [offsets[k], offsets[k+1]) -- advanced together, one launch per
+ * stage.  Each system has its own bounding box, Morton keys, octree and
+ * softening (softening[k]; NULL uses cfg->softening), and never feels the
+ * others: its result equals stepping it alone.  At most 512 systems and
+ * 2^25 particles.  The handle accepts every nbb_sim_* call. */
+int nbb_ensemble_create(const nbb_config *cfg, int n_systems,
+                        const int64_t *offsets, const double *softening,
+                        const double *mass, const double *x, const double *y,
+                        const double *z, const double *vx, const double *vy,
+                        const double *vz, int on_device, nbb_sim **out);
+
 /* Simulation::initialize (src/simulation.cpp:294-314): first spatial build
  * and acceleration; NBB_ERR_LOGIC when called twice. */
 int nbb_sim_initialize(nbb_sim *sim);
@@ -250,6 +263,12 @@ int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z,
                             size_t n, uint32_t *keys, uint32_t *idx,
                             void *stream);
 const char *nbb_noalloc_last_error_message(void);
+
+/* Self-test of failure detection: runs a device look-back whose predecessor
+ * never publishes.  The bounded spin gives up (about a second) and the call
+ * returns NBB_ERR_TIMEOUT with the CUDA context intact; any other status is a
+ * failure of the detection itself. */
+int nbb_selftest_bounded_wait(void);
 
 /* Last error of the calling thread. */
 const char *nbb_last_error_message(void);

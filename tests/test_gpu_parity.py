@@ -458,3 +458,21 @@ def test_full_size_invariants(nbb_mod):
     a = np.stack([out["ax"], out["ay"], out["az"]])[:, tg]
     rel = np.linalg.norm(a - exact, axis=0) / np.linalg.norm(exact, axis=0)
     assert float(np.sqrt(np.mean(rel ** 2))) < 1e-2
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(nbb_mod):
+    """A look-back whose predecessor never publishes ends with
+    NBB_ERR_TIMEOUT instead of hanging, and the GPU stays usable."""
+    import time
+
+    lib = nbb_mod.load()
+    t0 = time.time()
+    st = lib.nbb_selftest_bounded_wait()
+    assert st == 6, lib.nbb_last_error_message()  # NBB_ERR_TIMEOUT
+    assert time.time() - t0 < 60
+    assert b"gave up" in lib.nbb_last_error_message()
+    from nbb import ics
+
+    p = ics.plummer(2000, seed=1)
+    ax, _, _ = nbb_mod.compute_accelerations(p, 0.5, 0.01, 1.0)
+    assert np.all(np.isfinite(ax))
