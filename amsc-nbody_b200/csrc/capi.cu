@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -338,6 +339,22 @@ cudaError_t stage_in(const T *src, size_t count, bool on_device, Allocation &al,
 
 // -------------------------------------------------------------- handle ---
 
+// Device storage of a recorded rollout: (x, v, a) every `every` steps, the
+// final state, one segment of recomputed positions and the reverse-mode
+// buffers.  Taken when the rollout starts, released with the handle or by
+// the next rollout.
+struct RolloutRecord {
+  Allocation al;
+  uint64_t steps = 0, every = 0, slots = 0;
+  double *ckpt = nullptr;         // slots x 9 x n: x y z vx vy vz ax ay az
+  double *final_state = nullptr;  // 9 x n
+  double *seg = nullptr;          // (every - 1) x 3 x n recomputed positions
+  double *g = nullptr;            // 7 x n: gx gy gz gvx gvy gvz gm
+  double4 *node_g = nullptr, *part_g = nullptr, *tgt_g = nullptr;
+  int *pparent = nullptr;
+  int2 *prange = nullptr;
+};
+
 struct nbb_sim {
   nbb_config cfg{};
   Workspace ws{};
@@ -352,6 +369,7 @@ struct nbb_sim {
   uint64_t graph_kernels = 0;
   int tuned_group_size = 0;
   double min_softening = 0.0;  // ensembles: smallest per-system softening
+  std::unique_ptr<RolloutRecord> rollout;
 };
 
 extern "C" {
@@ -645,6 +663,15 @@ static cudaError_t capture_step(nbb_sim *sim) {
   return cudaSuccess;
 }
 
+// One step on the handle's stream: the captured graph, or the same kernels.
+static cudaError_t enqueue_step(nbb_sim *sim) {
+  if (sim->step_graph) {
+    nbb::count_launches(sim->graph_kernels);
+    return cudaGraphLaunch(sim->step_graph, sim->stream);
+  }
+  return enqueue_rebuild_force(sim->ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->stream);
+}
+
 static int run_steps(nbb_sim *sim, uint64_t steps, const char *what) {
   if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
   if (sim->state != nbb_sim::State::ready) return fail(NBB_ERR_LOGIC, what);
@@ -652,14 +679,7 @@ static int run_steps(nbb_sim *sim, uint64_t steps, const char *what) {
   Workspace &ws = sim->ws;
   cudaError_t e = cudaSuccess;
   if (steps > 0 && sim->cfg.use_graph && !sim->step_graph) e = capture_step(sim);
-  for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) {
-    if (sim->step_graph) {
-      e = cudaGraphLaunch(sim->step_graph, sim->stream);
-      nbb::count_launches(sim->graph_kernels);
-    } else {
-      e = enqueue_rebuild_force(ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->stream);
-    }
-  }
+  for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) e = enqueue_step(sim);
   if (e != cudaSuccess) {
     sim->state = nbb_sim::State::failed;
     return cuda_fail(e, "step");
@@ -1055,6 +1075,352 @@ int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right, int *rfir
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   cudaStreamDestroy(s);
   if (e != cudaSuccess) return cuda_fail(e, "buildTreeKernel execution");
+  return ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------- adjoint ----
+
+namespace {
+
+constexpr int kStateArrays = 9;
+
+double *const *state_arrays(Workspace &ws, double *(&arr)[kStateArrays]) {
+  double *a[kStateArrays] = {ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz, ws.ax, ws.ay, ws.az};
+  for (int k = 0; k < kStateArrays; ++k) arr[k] = a[k];
+  return arr;
+}
+
+// Copy the first `count` state arrays between the workspace and a slot of
+// contiguous n-arrays (save: workspace -> slot).
+cudaError_t copy_state(nbb_sim *sim, double *slot, int count, bool save) {
+  Workspace &ws = sim->ws;
+  double *arr[kStateArrays];
+  state_arrays(ws, arr);
+  const size_t n = (size_t)ws.n, bytes = n * sizeof(double);
+  for (int k = 0; k < count; ++k) {
+    double *dst = save ? slot + k * n : arr[k];
+    const double *src = save ? arr[k] : slot + k * n;
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, sim->stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Rebuild the tree on the workspace positions and add the VJP of the plain
+// FP64 force there to the cotangents.
+cudaError_t enqueue_vjp(nbb_sim *sim, const TraversalParams &tpa, const AdjointBuffers &ab) {
+  Workspace &ws = sim->ws;
+  cudaStream_t s = sim->stream;
+  cudaError_t e = launch_step_reset(ws, s);
+  if (e == cudaSuccess) e = launch_kd_bbox(ws, 0.0, 0, s);
+  if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
+  if (e == cudaSuccess) e = launch_tree(ws, tpa.theta, s);
+  if (e == cudaSuccess) e = launch_adjoint_force(ws, tpa, ab, s);
+  return e;
+}
+
+cudaMemcpyKind copy_kind(int on_device, bool to_device) {
+  if (on_device) return cudaMemcpyDeviceToDevice;
+  return to_device ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nbb_sim_rollout(nbb_sim *sim, uint64_t steps, uint64_t checkpoint_every) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (sim->state != nbb_sim::State::ready)
+    return fail(NBB_ERR_LOGIC, "Simulation must be initialized before a rollout");
+  if (checkpoint_every == 0) return fail(NBB_ERR_INVALID_ARGUMENT, "checkpoint interval must be positive");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  Workspace &ws = sim->ws;
+  const size_t n = (size_t)ws.n;
+  const uint64_t slots = steps == 0 ? 1 : (steps - 1) / checkpoint_every + 1;
+  const uint64_t seg = std::min<uint64_t>(checkpoint_every, steps > 0 ? steps : 1) - 1;
+  const double need = 8.0 * (double)n * (kStateArrays * (double)(slots + 1) + 3.0 * (double)seg + 7.0);
+  if (need > 0x1p46) return fail(NBB_ERR_INVALID_ARGUMENT, "rollout checkpoints exceed device memory");
+  sim->rollout.reset();
+  auto rec = std::make_unique<RolloutRecord>();
+  Allocation &al = rec->al;
+  cudaError_t e = al.get(rec->ckpt, (size_t)slots * kStateArrays * n);
+  if (e == cudaSuccess) e = al.get(rec->final_state, kStateArrays * n);
+  if (e == cudaSuccess) e = al.get(rec->seg, (size_t)(seg > 0 ? seg : 1) * 3 * n);
+  if (e == cudaSuccess) e = al.get(rec->g, 7 * n);
+  if (e == cudaSuccess) e = al.get(rec->node_g, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(rec->part_g, n);
+  if (e == cudaSuccess) e = al.get(rec->tgt_g, n);
+  if (e == cudaSuccess) e = al.get(rec->pparent, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(rec->prange, (size_t)ws.cap_nodes);
+  if (e != cudaSuccess) return cuda_fail(e, "rollout checkpoint allocation");
+  if (steps > 0 && sim->cfg.use_graph && !sim->step_graph) e = capture_step(sim);
+  if (e == cudaSuccess) e = copy_state(sim, rec->ckpt, kStateArrays, true);
+  for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+    e = enqueue_step(sim);
+    if (e == cudaSuccess && (k + 1) % checkpoint_every == 0 && k + 1 < steps)
+      e = copy_state(sim, rec->ckpt + (size_t)((k + 1) / checkpoint_every) * kStateArrays * n, kStateArrays,
+                     true);
+  }
+  if (e != cudaSuccess) {
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "rollout");
+  }
+  const int st = check_device(ws, sim->stream);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  rec->steps = steps;
+  rec->every = checkpoint_every;
+  rec->slots = slots;
+  sim->rollout = std::move(rec);
+  sim->time += sim->cfg.time_step * (double)steps;
+  sim->steps += steps;
+  return ok();
+}
+
+int nbb_sim_backward(nbb_sim *sim, const double *gx, const double *gy, const double *gz, const double *gvx,
+                     const double *gvy, const double *gvz, double *gm, double *gx0, double *gy0, double *gz0,
+                     double *gvx0, double *gvy0, double *gvz0, int on_device) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (sim->state != nbb_sim::State::ready)
+    return fail(NBB_ERR_LOGIC, "Simulation must be initialized before a backward pass");
+  if (!sim->rollout) return fail(NBB_ERR_LOGIC, "backward pass without a recorded rollout");
+  if (!gx || !gy || !gz) return fail(NBB_ERR_INVALID_ARGUMENT, "final-position cotangents are required");
+  if ((gvx || gvy || gvz) && !(gvx && gvy && gvz))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "velocity cotangents must be all given or all null");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  Workspace &ws = sim->ws;
+  RolloutRecord &rec = *sim->rollout;
+  cudaStream_t s = sim->stream;
+  const size_t n = (size_t)ws.n, bytes = n * sizeof(double);
+  double *G[7];
+  for (int k = 0; k < 7; ++k) G[k] = rec.g + k * n;
+  const double *gin[6] = {gx, gy, gz, gvx, gvy, gvz};
+  for (int k = 0; k < 6; ++k) {
+    if (gin[k]) {
+      NBB_CUDA(cudaMemcpyAsync(G[k], gin[k], bytes, copy_kind(on_device, true), s), "copy cotangents");
+    } else {
+      NBB_CUDA(cudaMemsetAsync(G[k], 0, bytes, s), "clear cotangents");
+    }
+  }
+  NBB_CUDA(cudaMemsetAsync(G[6], 0, bytes, s), "clear cotangents");
+  const uint64_t S = rec.steps, K = rec.every;
+  const double dt = sim->cfg.time_step;
+  AdjointBuffers ab;
+  ab.gx = G[0];
+  ab.gy = G[1];
+  ab.gz = G[2];
+  ab.gvx = G[3];
+  ab.gvy = G[4];
+  ab.gvz = G[5];
+  ab.gm = G[6];
+  ab.node_g = rec.node_g;
+  ab.part_g = rec.part_g;
+  ab.tgt_g = rec.tgt_g;
+  ab.pparent = rec.pparent;
+  ab.prange = rec.prange;
+  TraversalParams tpa = traversal_params(sim, 0);
+  tpa.precision = 0;
+  tpa.kick = 0;
+  tpa.group_mode = ws.n_systems > 1 ? 1 : 0;
+  cudaError_t e = cudaSuccess;
+  if (S > 0) {
+    // the step s -> s+1 is undone by the VJP at x_{s+1} with accelerations
+    // cotangent (1/2 dt at the last step, dt inside) times gv, then gv += dt gx
+    e = copy_state(sim, rec.final_state, kStateArrays, true);
+    for (uint64_t j = rec.slots; j-- > 0 && e == cudaSuccess;) {
+      const uint64_t lo = j * K, hi = std::min(lo + K, S);
+      e = copy_state(sim, rec.ckpt + (size_t)j * kStateArrays * n, kStateArrays, false);
+      for (uint64_t t = lo + 1; t < hi && e == cudaSuccess; ++t) {
+        e = enqueue_step(sim);
+        if (e == cudaSuccess) e = copy_state(sim, rec.seg + (size_t)(t - lo - 1) * 3 * n, 3, true);
+      }
+      for (uint64_t t = hi; t > lo && e == cudaSuccess; --t) {
+        double *pos = (t < hi) ? rec.seg + (size_t)(t - lo - 1) * 3 * n
+                               : (hi == S ? rec.final_state : rec.ckpt + (size_t)(j + 1) * kStateArrays * n);
+        e = copy_state(sim, pos, 3, false);
+        ab.coef = (t == S) ? 0.5 * dt : dt;
+        ab.dt_v = dt;
+        if (e == cudaSuccess) e = enqueue_vjp(sim, tpa, ab);
+      }
+    }
+    if (e == cudaSuccess) e = copy_state(sim, rec.ckpt, 3, false);
+    ab.coef = 0.5 * dt;  // a_0 = F(x_0) enters through the first half kick only
+    ab.dt_v = 0.0;
+    if (e == cudaSuccess) e = enqueue_vjp(sim, tpa, ab);
+    if (e == cudaSuccess) e = copy_state(sim, rec.final_state, kStateArrays, false);
+  }
+  if (e != cudaSuccess) {
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "backward pass");
+  }
+  const int st = check_device(ws, s);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  double *outs[7] = {gx0, gy0, gz0, gvx0, gvy0, gvz0, gm};
+  for (int k = 0; k < 7; ++k)
+    if (outs[k]) NBB_CUDA(cudaMemcpyAsync(outs[k], G[k], bytes, copy_kind(on_device, false), s), "copy gradients");
+  NBB_CUDA(cudaStreamSynchronize(s), "backward synchronisation");
+  return ok();
+}
+
+int nbb_frozen_rollout(const nbb_config *cfg, size_t n, const double *mass, const double *x, const double *y,
+                       const double *z, const double *vx, const double *vy, const double *vz, size_t copies,
+                       const double *cmass, const double *cx, const double *cy, const double *cz,
+                       const double *cvx, const double *cvy, const double *cvz, uint64_t steps, double *ox,
+                       double *oy, double *oz, double *ovx, double *ovy, double *ovz, int on_device) {
+  if (!cfg) return fail(NBB_ERR_INVALID_ARGUMENT, "null configuration");
+  if (copies == 0 || copies > 4096) return fail(NBB_ERR_INVALID_ARGUMENT, "copies must be in [1, 4096]");
+  if (!cx || !cy || !cz || !cvx || !cvy || !cvz)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "perturbed positions and velocities are required");
+  nbb_config c2 = *cfg;
+  c2.precision = NBB_PRECISION_FP64;
+  c2.use_graph = 0;
+  nbb_sim *sim = nullptr;
+  int st = create_sim(&c2, n, 1, nullptr, nullptr, mass, x, y, z, vx, vy, vz, nullptr, on_device, &sim);
+  if (st) return st;
+  std::unique_ptr<nbb_sim, int (*)(nbb_sim *)> guard(sim, nbb_sim_destroy);
+  st = nbb_sim_initialize(sim);
+  if (st) return st;
+  Workspace &ws = sim->ws;
+  cudaStream_t s = sim->stream;
+  const size_t bytes = n * sizeof(double);
+  Allocation al;
+  std::vector<FrozenCopy> cp(copies);
+  double4 *pm4q = nullptr, *node_aq = nullptr;
+  int *pparent = nullptr;
+  int2 *prange = nullptr;
+  cudaError_t e = al.get(pm4q, n);
+  if (e == cudaSuccess) e = al.get(node_aq, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(pparent, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(prange, (size_t)ws.cap_nodes);
+  const double *src[7] = {cmass, cx, cy, cz, cvx, cvy, cvz};
+  for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
+    double *arr[10];
+    for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = al.get(arr[k], n);
+    if (e != cudaSuccess) break;
+    FrozenCopy &c = cp[q];
+    c.m = arr[0]; c.x = arr[1]; c.y = arr[2]; c.z = arr[3];
+    c.vx = arr[4]; c.vy = arr[5]; c.vz = arr[6];
+    c.ax = arr[7]; c.ay = arr[8]; c.az = arr[9];
+    for (int k = 0; k < 7 && e == cudaSuccess; ++k) {
+      if (src[k])
+        e = cudaMemcpyAsync(arr[k], src[k] + q * n, bytes, copy_kind(on_device, true), s);
+      else
+        e = cudaMemcpyAsync(arr[k], ws.m, bytes, cudaMemcpyDeviceToDevice, s);
+    }
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "frozen rollout setup");
+  const TraversalParams tp = traversal_params(sim, 0);
+  const double dt = c2.time_step;
+  e = launch_frozen_topology(ws, pparent, prange, s);
+  for (size_t q = 0; q < copies && e == cudaSuccess; ++q)
+    e = launch_frozen_force(ws, tp, cp[q], prange, pm4q, node_aq, s);
+  for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) {
+    for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
+      const FrozenCopy &c = cp[q];
+      e = launch_kick_drift(c.x, c.y, c.z, c.vx, c.vy, c.vz, c.ax, c.ay, c.az, n, dt, s);
+    }
+    if (e == cudaSuccess) e = enqueue_rebuild_force(ws, traversal_params(sim, 1), dt, 1, s);
+    if (e == cudaSuccess) e = launch_frozen_topology(ws, pparent, prange, s);
+    for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
+      const FrozenCopy &c = cp[q];
+      e = launch_frozen_force(ws, tp, c, prange, pm4q, node_aq, s);
+      if (e == cudaSuccess) e = launch_kick(c.vx, c.vy, c.vz, c.ax, c.ay, c.az, n, dt, s);
+    }
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "frozen rollout");
+  st = check_device(ws, s);
+  if (st) return st;
+  double *outs[6] = {ox, oy, oz, ovx, ovy, ovz};
+  for (size_t q = 0; q < copies; ++q) {
+    const double *from[6] = {cp[q].x, cp[q].y, cp[q].z, cp[q].vx, cp[q].vy, cp[q].vz};
+    for (int k = 0; k < 6; ++k)
+      if (outs[k])
+        NBB_CUDA(cudaMemcpyAsync(outs[k] + q * n, from[k], bytes, copy_kind(on_device, false), s),
+                 "copy frozen rollout state");
+  }
+  NBB_CUDA(cudaStreamSynchronize(s), "frozen rollout synchronisation");
+  return ok();
+}
+
+int nbb_direct_rollout_adjoint(const nbb_config *cfg, size_t n, const double *mass, const double *x,
+                               const double *y, const double *z, const double *vx, const double *vy,
+                               const double *vz, uint64_t steps, const double *gx, const double *gy,
+                               const double *gz, const double *gvx, const double *gvy, const double *gvz,
+                               double *ox, double *oy, double *oz, double *ovx, double *ovy, double *ovz,
+                               double *gm, double *gx0, double *gy0, double *gz0, double *gvx0, double *gvy0,
+                               double *gvz0, int on_device) {
+  if (!cfg) return fail(NBB_ERR_INVALID_ARGUMENT, "null configuration");
+  int st = validate_config(cfg);
+  if (st) return st;
+  if (n == 0 || n > (size_t)INT_MAX) return fail(NBB_ERR_INVALID_ARGUMENT, "particle count out of range");
+  if (!mass || !x || !y || !z || !vx || !vy || !vz || !gx || !gy || !gz)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "state and final-position cotangents are required");
+  if ((gvx || gvy || gvz) && !(gvx && gvy && gvz))
+    return fail(NBB_ERR_INVALID_ARGUMENT, "velocity cotangents must be all given or all null");
+  const double need = 8.0 * (double)n * (3.0 * (double)(steps + 1) + 17.0);
+  if (need > 0x1p34) return fail(NBB_ERR_INVALID_ARGUMENT, "the direct adjoint's stored trajectory exceeds 16 GiB");
+  NBB_CUDA(cudaSetDevice(cfg->device), "cudaSetDevice");
+  cudaStream_t s = nullptr;
+  NBB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  std::unique_ptr<CUstream_st, cudaError_t (*)(cudaStream_t)> sguard(s, cudaStreamDestroy);
+  Allocation al;
+  const size_t bytes = n * sizeof(double);
+  double *traj = nullptr, *st10 = nullptr, *g = nullptr;
+  cudaError_t e = al.get(traj, (size_t)(steps + 1) * 3 * n);
+  if (e == cudaSuccess) e = al.get(st10, 10 * n);
+  if (e == cudaSuccess) e = al.get(g, 7 * n);
+  if (e != cudaSuccess) return cuda_fail(e, "direct adjoint allocation");
+  double *M = st10, *X = st10 + n, *Y = st10 + 2 * n, *Z = st10 + 3 * n, *VX = st10 + 4 * n,
+         *VY = st10 + 5 * n, *VZ = st10 + 6 * n, *AX = st10 + 7 * n, *AY = st10 + 8 * n, *AZ = st10 + 9 * n;
+  const double *in[7] = {mass, x, y, z, vx, vy, vz};
+  double *dst[7] = {M, X, Y, Z, VX, VY, VZ};
+  for (int k = 0; k < 7; ++k)
+    NBB_CUDA(cudaMemcpyAsync(dst[k], in[k], bytes, copy_kind(on_device, true), s), "copy state");
+  const double dt = cfg->time_step, G = cfg->gravitational_constant, eps = cfg->softening;
+  auto store = [&](uint64_t t) -> cudaError_t {
+    double *slot = traj + (size_t)t * 3 * n;
+    cudaError_t r = cudaMemcpyAsync(slot, X, bytes, cudaMemcpyDeviceToDevice, s);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(slot + n, Y, bytes, cudaMemcpyDeviceToDevice, s);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(slot + 2 * n, Z, bytes, cudaMemcpyDeviceToDevice, s);
+    return r;
+  };
+  e = store(0);
+  if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, s);
+  for (uint64_t t = 1; t <= steps && e == cudaSuccess; ++t) {
+    e = launch_kick_drift(X, Y, Z, VX, VY, VZ, AX, AY, AZ, n, dt, s);
+    if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, s);
+    if (e == cudaSuccess) e = launch_kick(VX, VY, VZ, AX, AY, AZ, n, dt, s);
+    if (e == cudaSuccess) e = store(t);
+  }
+  double *Gc[7];
+  for (int k = 0; k < 7; ++k) Gc[k] = g + k * n;
+  const double *gin[6] = {gx, gy, gz, gvx, gvy, gvz};
+  for (int k = 0; k < 6 && e == cudaSuccess; ++k)
+    e = gin[k] ? cudaMemcpyAsync(Gc[k], gin[k], bytes, copy_kind(on_device, true), s)
+               : cudaMemsetAsync(Gc[k], 0, bytes, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(Gc[6], 0, bytes, s);
+  for (uint64_t t = steps; t >= 1 && e == cudaSuccess; --t) {
+    const double *slot = traj + (size_t)t * 3 * n;
+    e = launch_direct_vjp(n, M, slot, slot + n, slot + 2 * n, Gc[3], Gc[4], Gc[5], t == steps ? 0.5 * dt : dt, G,
+                          eps, Gc[0], Gc[1], Gc[2], Gc[6], s);
+    if (e == cudaSuccess) e = launch_axpy3(Gc[3], Gc[4], Gc[5], Gc[0], Gc[1], Gc[2], dt, n, s);
+  }
+  if (steps > 0 && e == cudaSuccess)
+    e = launch_direct_vjp(n, M, traj, traj + n, traj + 2 * n, Gc[3], Gc[4], Gc[5], 0.5 * dt, G, eps, Gc[0], Gc[1],
+                          Gc[2], Gc[6], s);
+  double *outs[13] = {ox, oy, oz, ovx, ovy, ovz, gx0, gy0, gz0, gvx0, gvy0, gvz0, gm};
+  const double *from[13] = {X, Y, Z, VX, VY, VZ, Gc[0], Gc[1], Gc[2], Gc[3], Gc[4], Gc[5], Gc[6]};
+  for (int k = 0; k < 13 && e == cudaSuccess; ++k)
+    if (outs[k]) e = cudaMemcpyAsync(outs[k], from[k], bytes, copy_kind(on_device, false), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "direct adjoint");
   return ok();
 }
 

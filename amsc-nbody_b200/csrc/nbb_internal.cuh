@@ -284,4 +284,42 @@ cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys,
 // Topology stages only (Karras .. materialise) for caller keys.
 cudaError_t launch_topology(Workspace &ws, cudaStream_t s);
 
+// Reverse-mode buffers of one frozen-structure force evaluation.  The
+// accelerations cotangent is coef * (gvx, gvy, gvz); gx / gy / gz / gm
+// accumulate; gv += dt_v * gx afterwards when dt_v != 0.
+struct AdjointBuffers {
+  double *gvx = nullptr, *gvy = nullptr, *gvz = nullptr;
+  double coef = 0.0;
+  double dt_v = 0.0;
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr, *gm = nullptr;
+  double4 *node_g = nullptr;  // per preorder node (cap_nodes)
+  double4 *part_g = nullptr;  // per Morton slot
+  double4 *tgt_g = nullptr;   // per Morton slot
+  int *pparent = nullptr;     // per preorder node
+  int2 *prange = nullptr;     // per preorder node
+};
+// A perturbed copy of the particles (original order).
+struct FrozenCopy {
+  double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
+  double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  double *ax = nullptr, *ay = nullptr, *az = nullptr;
+};
+// VJP of the plain FP64 force on the current tree (built from the positions
+// in the workspace): accumulates into ab.gx / gy / gz / gm.
+cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,
+                                 cudaStream_t s);
+// Preorder parents and particle ranges of the current tree.
+cudaError_t launch_frozen_topology(Workspace &ws, int *pparent, int2 *prange, cudaStream_t s);
+// Force on a perturbed copy with the current tree's structure (accelerations
+// into c.ax / ay / az).
+cudaError_t launch_frozen_force(Workspace &ws, const TraversalParams &p, const FrozenCopy &c,
+                                const int2 *prange, double4 *pm4q, double4 *node_aq, cudaStream_t s);
+// Adjoint of the FP64 direct sum (accumulating).
+cudaError_t launch_direct_vjp(size_t n, const double *m, const double *x, const double *y, const double *z,
+                              const double *gvx, const double *gvy, const double *gvz, double coef, double g,
+                              double soft, double *gx, double *gy, double *gz, double *gm, cudaStream_t s);
+// y += a x on three arrays.
+cudaError_t launch_axpy3(double *yx, double *yy, double *yz, const double *xx, const double *xy, const double *xz,
+                         double a, size_t n, cudaStream_t s);
+
 }  // namespace nbb

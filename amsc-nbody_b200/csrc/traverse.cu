@@ -11,6 +11,7 @@
 //                         node numbering (function-level API).
 //  kick / kick_drift      integrator.cu:57-112.
 #include "nbb_internal.cuh"
+#include "walk_fp64.cuh"
 
 #include <climits>
 #include <cmath>
@@ -20,26 +21,6 @@ namespace nbb {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-
-// barnes_hut.cu:76-100: G m (d^2 + eps^2)^-3/2 d, accumulated with the
-// reference's operation order.  Returns false on a singular interaction.
-__device__ __forceinline__ bool point_mass_fp64(double dx, double dy, double dz, double d2,
-                                                double m, double g, double soft2, double &ax,
-                                                double &ay, double &az) {
-  const double r2 = __dadd_rn(d2, soft2);
-  if (r2 <= 0.0) return false;
-  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
-  const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
-  const double f = __dmul_rn(__dmul_rn(g, m), inv3);
-  ax = __fma_rn(f, dx, ax);
-  ay = __fma_rn(f, dy, ay);
-  az = __fma_rn(f, dz, az);
-  return true;
-}
-
-__device__ __forceinline__ double sqdist(double dx, double dy, double dz) {
-  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
-}
 
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -110,17 +91,9 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
         } else if (a.w == 0.0) {
           resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
         } else {
-          const double dx = __dsub_rn(a.x, t.x), dy = __dsub_rn(a.y, t.y), dz = __dsub_rn(a.z, t.z);
-          const double d2 = sqdist(dx, dy, dz);
-          // sqrt(d2) > crit, decided on d2 vs crit^2 outside a 2^-44 band
-          bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
+          double dx, dy, dz, d2;
+          const bool accept = accept_fp64(a, b, c, t, dx, dy, dz, d2);
           ++tests;
-          if (accept) {
-            const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w &&
-                                  fabs(__dsub_rn(t.y, b.y)) <= b.w &&
-                                  fabs(__dsub_rn(t.z, b.z)) <= b.w;
-            accept = !contains && d2 > 0.0;
-          }
           if (accept) {
             singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
             ++inter;

@@ -1,0 +1,51 @@
+// walk_fp64.cuh -- FP64 interaction and acceptance test shared by the plain
+// force walk, the frozen-structure replay and the adjoint walk, so all three
+// take the same decisions on the same inputs.
+#pragma once
+
+#include "nbb_internal.cuh"
+
+namespace nbb {
+
+// barnes_hut.cu:76-100: G m (d^2 + eps^2)^-3/2 d, accumulated with the
+// reference's operation order.  Returns false on a singular interaction.
+__device__ __forceinline__ bool point_mass_fp64(double dx, double dy, double dz, double d2,
+                                                double m, double g, double soft2, double &ax,
+                                                double &ay, double &az) {
+  const double r2 = __dadd_rn(d2, soft2);
+  if (r2 <= 0.0) return false;
+  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
+  const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
+  const double f = __dmul_rn(__dmul_rn(g, m), inv3);
+  ax = __fma_rn(f, dx, ax);
+  ay = __fma_rn(f, dy, ay);
+  az = __fma_rn(f, dz, az);
+  return true;
+}
+
+__device__ __forceinline__ double sqdist(double dx, double dy, double dz) {
+  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+}
+
+// barnes_hut.cu:292-322: the acceptance test of target t at a node with
+// records a = (com, mass), b = (centre, half size), c = (crit, crit^2 band).
+// sqrt(d2) > crit is decided on d2 against crit^2 outside a 2^-44 band and by
+// the exact square root inside it; a node containing the target, or at zero
+// distance, is never accepted.  Returns the offset com - t and its square.
+__device__ __forceinline__ bool accept_fp64(const double4 &a, const double4 &b, const double4 &c,
+                                            const double4 &t, double &dx, double &dy, double &dz,
+                                            double &d2) {
+  dx = __dsub_rn(a.x, t.x);
+  dy = __dsub_rn(a.y, t.y);
+  dz = __dsub_rn(a.z, t.z);
+  d2 = sqdist(dx, dy, dz);
+  bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
+  if (accept) {
+    const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w && fabs(__dsub_rn(t.y, b.y)) <= b.w &&
+                          fabs(__dsub_rn(t.z, b.z)) <= b.w;
+    accept = !contains && d2 > 0.0;
+  }
+  return accept;
+}
+
+}  // namespace nbb

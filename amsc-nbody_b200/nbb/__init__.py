@@ -9,8 +9,8 @@ marshals arguments.
 from ._lib import (PRECISION_FP64, PRECISION_MIXED, DeviceError, DomainError, InvalidArgument,
                    LogicError, NbbError, NoDevice, OverflowErrorNbb, load)
 from .api import (G_SI, BarnesHutParameters, EnsembleSimulation, Simulation, SimulationConfig, compute_accelerations,
-                  compute_direct_accelerations, computeBarnesHutAcceleration, kernel_launch_count,
-                  measure_fma_tflops,
+                  compute_direct_accelerations, computeBarnesHutAcceleration, direct_rollout_adjoint,
+                  frozen_rollout, kernel_launch_count, measure_fma_tflops,
                   leapfrog_kick, leapfrog_kick_drift, node_capacity, octree_from_keys, radix_tree)
 from .ics import ParticleData
 
@@ -18,8 +18,8 @@ __all__ = [
     "PRECISION_FP64", "PRECISION_MIXED", "DeviceError", "DomainError", "InvalidArgument",
     "LogicError", "NbbError", "NoDevice", "OverflowErrorNbb", "load", "G_SI",
     "BarnesHutParameters", "EnsembleSimulation", "Simulation", "SimulationConfig", "compute_accelerations",
-    "compute_direct_accelerations", "computeBarnesHutAcceleration", "kernel_launch_count",
-    "measure_fma_tflops",
+    "compute_direct_accelerations", "computeBarnesHutAcceleration", "direct_rollout_adjoint",
+    "frozen_rollout", "kernel_launch_count", "measure_fma_tflops",
     "leapfrog_kick", "leapfrog_kick_drift", "node_capacity", "octree_from_keys", "radix_tree",
     "ParticleData",
 ]

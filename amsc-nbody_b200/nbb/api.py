@@ -148,6 +148,31 @@ class Simulation:
         check(self._lib.nbb_sim_profile(self._handle, ms, C.byref(st)))
         return dict(zip(self.PROFILE_STAGES, list(ms))), st
 
+    def rollout(self, steps: int, checkpoint_every: int = 32) -> None:
+        """Advance ``steps`` steps keeping (x, v, a) every
+        ``checkpoint_every`` steps for :meth:`backward` (nbb_sim_rollout)."""
+        check(self._lib.nbb_sim_rollout(self._handle, int(steps), int(checkpoint_every)))
+
+    def backward(self, grad_positions, grad_velocities=None):
+        """Gradient of a loss of the last rollout's final state with respect
+        to its initial state (nbb_sim_backward).  ``grad_positions`` /
+        ``grad_velocities`` are dL/d(final x, y, z) and dL/d(final vx, vy, vz)
+        as three arrays (or a (3, n) array).  Returns (grad_mass,
+        grad_positions (3, n), grad_velocities (3, n))."""
+        n = self._n
+        gp = [_f64(a) for a in grad_positions]
+        gv = None if grad_velocities is None else [_f64(a) for a in grad_velocities]
+        if len(gp) != 3 or any(a.size != n for a in gp) or (gv is not None and (
+                len(gv) != 3 or any(a.size != n for a in gv))):
+            raise _lib.InvalidArgument(_lib.ERR_INVALID_ARGUMENT, "cotangents must be three arrays of n values")
+        gm = np.empty(n)
+        gx0 = np.empty((3, n))
+        gv0 = np.empty((3, n))
+        gvp = [None] * 3 if gv is None else [ptr(a) for a in gv]
+        check(self._lib.nbb_sim_backward(self._handle, *[ptr(a) for a in gp], *gvp, ptr(gm),
+                                         *[ptr(gx0[k]) for k in range(3)], *[ptr(gv0[k]) for k in range(3)], 0))
+        return gm, gx0, gv0
+
     def export_tree(self, m_capacity: int | None = None) -> dict:
         return _export(lambda e: self._lib.nbb_sim_export(self._handle, C.byref(e)), self._n, m_capacity)
 
@@ -347,3 +372,46 @@ def measure_fma_tflops(precision: int) -> float:
 
 def kernel_launch_count() -> int:
     return int(_lib.load().nbb_kernel_launch_count())
+
+
+def frozen_rollout(particles: ParticleData, config: SimulationConfig, copies, steps: int):
+    """Final states of perturbed copies advanced with the unperturbed
+    system's tree structure at every step (nbb_frozen_rollout).  ``copies``
+    is a sequence of ParticleData of the same size; returns an array
+    (copies, 6, n) of final x, y, z, vx, vy, vz."""
+    lib = _lib.load()
+    n = len(particles)
+    base = [_f64(a) for a in particles.arrays()]
+    q = len(copies)
+    stack = [np.ascontiguousarray(np.stack([getattr(c, f) for c in copies]), dtype=np.float64)
+             for f in ("mass", "x", "y", "z", "vx", "vy", "vz")]
+    if any(a.shape != (q, n) for a in stack):
+        raise _lib.InvalidArgument(_lib.ERR_INVALID_ARGUMENT, "every copy must hold n particles")
+    out = np.empty((6, q, n))
+    cfg = config.to_c()
+    check(lib.nbb_frozen_rollout(C.byref(cfg), n, *[ptr(a) for a in base], q, *[ptr(a) for a in stack],
+                                 int(steps), *[ptr(out[k]) for k in range(6)], 0))
+    return np.ascontiguousarray(out.transpose(1, 0, 2))
+
+
+def direct_rollout_adjoint(particles: ParticleData, config: SimulationConfig, steps: int, grad_positions,
+                           grad_velocities=None):
+    """FP64 direct-summation rollout and its adjoint
+    (nbb_direct_rollout_adjoint).  Returns (final state (6, n), grad_mass,
+    grad_positions (3, n), grad_velocities (3, n))."""
+    lib = _lib.load()
+    n = len(particles)
+    arrs = [_f64(a) for a in particles.arrays()]
+    gp = [_f64(a) for a in grad_positions]
+    keep = None if grad_velocities is None else [_f64(a) for a in grad_velocities]
+    gvp = [None] * 3 if keep is None else [ptr(a) for a in keep]
+    final = np.empty((6, n))
+    gm = np.empty(n)
+    gx0 = np.empty((3, n))
+    gv0 = np.empty((3, n))
+    cfg = config.to_c()
+    check(lib.nbb_direct_rollout_adjoint(C.byref(cfg), n, *[ptr(a) for a in arrs], int(steps),
+                                         *[ptr(a) for a in gp], *gvp, *[ptr(final[k]) for k in range(6)],
+                                         ptr(gm), *[ptr(gx0[k]) for k in range(3)],
+                                         *[ptr(gv0[k]) for k in range(3)], 0))
+    return final, gm, gx0, gv0

@@ -270,6 +270,58 @@ const char *nbb_noalloc_last_error_message(void);
  * failure of the detection itself. */
 int nbb_selftest_bounded_wait(void);
 
+/* ---------------------------------------------------------------------------
+ * Differentiable rollout.  No counterpart in the reference (which has no
+ * derivative of its step); the force differentiated is the plain FP64
+ * Barnes-Hut force of src/barnes_hut.cu:184-342 with the tree topology and
+ * every target's accepted-node and opened-leaf sets held fixed at the
+ * positions of each step.
+ *
+ * nbb_sim_rollout advances an initialized simulation by `steps` steps (as
+ * nbb_sim_run) and keeps (x, v, a) every `checkpoint_every` steps on the
+ * device.  nbb_sim_backward then returns the gradient of a scalar loss of the
+ * final state with respect to the rollout's initial masses, positions and
+ * velocities, given dL/d(final positions) and, optionally (all three or none),
+ * dL/d(final velocities).  It recomputes each checkpoint segment forward with
+ * the handle's own step (so a mixed-precision rollout is differentiated along
+ * its own trajectory), rebuilds the tree at every stored position and applies
+ * the hand-written vector-Jacobian product of the force and of the leapfrog
+ * kick-drift-kick.  The handle's state is restored to the rollout's final
+ * state before returning.  Output pointers may be null (not copied); on_device
+ * says whether every array argument is a device pointer.
+ * ------------------------------------------------------------------------- */
+int nbb_sim_rollout(nbb_sim *sim, uint64_t steps, uint64_t checkpoint_every);
+int nbb_sim_backward(nbb_sim *sim, const double *gx, const double *gy, const double *gz, const double *gvx,
+                     const double *gvy, const double *gvz, double *gm, double *gx0, double *gy0, double *gz0,
+                     double *gvx0, double *gvy0, double *gvz0, int on_device);
+
+/* Frozen-structure replay, for finite differences of the differentiated
+ * function: the unperturbed system (m, x, y, z, vx, vy, vz; FP64 plain
+ * stepping) advances `steps` steps, and alongside it `copies` perturbed
+ * copies (copy q at offset q*n of each c* array; cmass may be null for the
+ * unperturbed masses) advance with forces evaluated on the unperturbed
+ * system's tree, acceptance decisions and leaf sets of the same step.  Writes
+ * each copy's final positions / velocities at offset q*n. */
+int nbb_frozen_rollout(const nbb_config *cfg, size_t n, const double *mass, const double *x, const double *y,
+                       const double *z, const double *vx, const double *vy, const double *vz, size_t copies,
+                       const double *cmass, const double *cx, const double *cy, const double *cz,
+                       const double *cvx, const double *cvy, const double *cvz, uint64_t steps, double *ox,
+                       double *oy, double *oz, double *ovx, double *ovy, double *ovz, int on_device);
+
+/* FP64 direct-summation rollout and its adjoint (the theta-error oracle of
+ * the tree adjoint): `steps` leapfrog steps with all-pairs forces (softening
+ * and G from cfg; theta, precision and group size ignored), final state into
+ * o* (each may be null), and the gradient with respect to the initial state
+ * for the final-state cotangents, as nbb_sim_backward.  Stores every step's
+ * positions (refused above 16 GiB). */
+int nbb_direct_rollout_adjoint(const nbb_config *cfg, size_t n, const double *mass, const double *x,
+                               const double *y, const double *z, const double *vx, const double *vy,
+                               const double *vz, uint64_t steps, const double *gx, const double *gy,
+                               const double *gz, const double *gvx, const double *gvy, const double *gvz,
+                               double *ox, double *oy, double *oz, double *ovx, double *ovy, double *ovz,
+                               double *gm, double *gx0, double *gy0, double *gz0, double *gvx0, double *gvy0,
+                               double *gvz0, int on_device);
+
 /* Last error of the calling thread. */
 const char *nbb_last_error_message(void);
 int nbb_last_error_code(void);
