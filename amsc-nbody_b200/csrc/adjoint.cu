@@ -27,9 +27,10 @@
 //                        (all lanes at a node share it) and added atomically
 //   adj_node_kernel      (gX, gM) -> (P, Q) per node
 //   adj_leaf_kernel      root-path sums, per-particle totals, velocity update
-//   frozen_*             the force on a perturbed copy of the particles with
+//   frozen_*             the force on perturbed copies of the particles with
 //                        the tree, acceptance decisions and leaf sets of the
-//                        unperturbed particles
+//                        unperturbed particles (all copies in one launch per
+//                        stage; node masses bottom-up, one launch per level)
 //   direct_vjp_kernel    adjoint of the FP64 direct sum (all pairs)
 #include "nbb_internal.cuh"
 #include "walk_fp64.cuh"
@@ -102,7 +103,8 @@ __global__ void adj_reset_kernel(DevScalars *sc) {
 
 // Preorder parent and Morton-order particle range of every octree node
 // (pre = sum of preorder offsets up the parent chain, as the layout does).
-__global__ void __launch_bounds__(kBlock) adj_topology_kernel(Workspace ws, int *pparent, int2 *prange) {
+__global__ void __launch_bounds__(kBlock) adj_topology_kernel(Workspace ws, int *pparent, int2 *prange,
+                                                              int *pre_of) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int m = sc->n_nodes;
@@ -117,6 +119,7 @@ __global__ void __launch_bounds__(kBlock) adj_topology_kernel(Workspace ws, int 
       record_error(sc, kStageLayout, 1);
       continue;
     }
+    if (pre_of) pre_of[v] = pre;
     pparent[pre] = (v == 0) ? -1 : pre - ws.preoff[v];
     const bool leaf = ws.child_count[v] == 0;
     const int cnt = leaf ? max(ws.ocount[v], 0) : ws.psub[v];
@@ -283,62 +286,84 @@ __global__ void __launch_bounds__(kBlock) adj_leaf_kernel(Workspace ws, AdjointB
 
 // ------------------------------------------------------------ frozen ----
 
-// Perturbed particles in the unperturbed Morton order.
-__global__ void frozen_gather_kernel(Workspace ws, FrozenCopy c, double4 *pm4q) {
-  for (int sp = blockIdx.x * blockDim.x + threadIdx.x; sp < ws.n; sp += gridDim.x * blockDim.x) {
-    const uint32_t j = ws.idx[sp];
-    pm4q[sp] = make_double4(c.x[j], c.y[j], c.z[j], c.m[j]);
+// Perturbed copies in the unperturbed Morton order (copy q at q * n).
+__global__ void frozen_gather_kernel(Workspace ws, FrozenBatch fb) {
+  const size_t n = (size_t)ws.n, total = n * (size_t)fb.copies;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+    const size_t q = k / n, sp = k - q * n;
+    const size_t j = q * n + ws.idx[sp];
+    fb.pm4q[k] = make_double4(fb.x[j], fb.y[j], fb.z[j], fb.m[j]);
   }
 }
 
-// Mass and centre of mass of the perturbed particles of every node (one warp
-// per node, fixed summation order).
-__global__ void __launch_bounds__(kBlock) frozen_mass_kernel(Workspace ws, const int2 *prange,
-                                                             const double4 *pm4q, double4 *node_aq) {
+// Mass and centre of mass of every copy's particles in each node of one
+// octree level (deepest level first): leaves sum their particles in Morton
+// order, internal nodes combine their children in octant order 0..7.  Values
+// are kept by octree id (for the parents) and written at the preorder id.
+__global__ void __launch_bounds__(kBlock) frozen_level_kernel(Workspace ws, FrozenBatch fb, int level) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
-  const int m = sc->n_nodes;
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  for (int pre = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pre < m; pre += warps) {
-    const int2 r = prange[pre];
+  const size_t m = (size_t)sc->n_nodes, cap = (size_t)ws.cap_nodes, n = (size_t)ws.n;
+  const size_t total = m * (size_t)fb.copies;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+    const size_t q = k / m;
+    const int v = (int)(k - q * m);
+    if (ws.olevel[v] != level) continue;
     double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    for (int k = lane; k < r.y; k += 32) {
-      const double4 q = pm4q[r.x + k];
-      tm += q.w;
-      wx = fma(q.w, q.x, wx);
-      wy = fma(q.w, q.y, wy);
-      wz = fma(q.w, q.z, wz);
+    if (ws.child_count[v] == 0) {
+      const int f = ws.ofirst[v], c = ws.ocount[v];
+      if (c > 0 && f >= 0 && (size_t)(f + c) <= n) {
+        const double4 *pq = fb.pm4q + q * n + f;
+        for (int i = 0; i < c; ++i) {
+          const double4 t = pq[i];
+          tm += t.w;
+          wx = fma(t.w, t.x, wx);
+          wy = fma(t.w, t.y, wy);
+          wz = fma(t.w, t.z, wz);
+        }
+      }
+    } else {
+      for (int o = 0; o < 8; ++o) {
+        const int c = ws.children[(size_t)v * 8 + o];
+        if (c <= 0 || (size_t)c >= m) continue;
+        const double4 t = fb.aq_oct[q * cap + c];
+        tm += t.w;
+        wx = fma(t.w, t.x, wx);
+        wy = fma(t.w, t.y, wy);
+        wz = fma(t.w, t.z, wz);
+      }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      tm += __shfl_xor_sync(kFull, tm, o);
-      wx += __shfl_xor_sync(kFull, wx, o);
-      wy += __shfl_xor_sync(kFull, wy, o);
-      wz += __shfl_xor_sync(kFull, wz, o);
-    }
-    if (lane == 0)
-      node_aq[pre] = (tm > 0.0) ? make_double4(wx / tm, wy / tm, wz / tm, tm) : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double4 r = (tm > 0.0) ? make_double4(wx / tm, wy / tm, wz / tm, tm) : make_double4(0.0, 0.0, 0.0, 0.0);
+    fb.aq_oct[q * cap + v] = r;
+    const int pre = fb.pre_of[v];
+    if (pre >= 0 && (size_t)pre < m) fb.node_aq[q * cap + pre] = r;
   }
 }
 
-// Force on the perturbed copy: visit order, acceptance decisions, zero-mass
+// Force on each perturbed copy: visit order, acceptance decisions, zero-mass
 // skips and self exclusion from the unperturbed tree and targets; offsets,
-// masses and centres of mass from the copy.
-__global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, TraversalParams p, const double4 *pm4q,
-                                                         const double4 *node_aq, FrozenCopy out) {
+// masses and centres of mass from the copy.  Work items are (copy, target
+// group) pairs taken from one counter, so every copy's walk shares the grid.
+__global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, TraversalParams p, FrozenBatch fb) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int lane = threadIdx.x & 31;
   const int n = ws.n;
   const int m = sc->n_nodes;
+  const size_t cap = (size_t)ws.cap_nodes;
   const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
+  const unsigned items = (unsigned)n_groups * (unsigned)fb.copies;
   const double g = p.g;
   bool singular = false;
   while (true) {
-    int grp = 0;
-    if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
-    grp = __shfl_sync(kFull, grp, 0);
-    if (grp >= n_groups) break;
+    unsigned item = 0;
+    if (lane == 0) item = atomicAdd(&sc->work_counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= items) break;
+    const int q = (int)(item / (unsigned)n_groups);
+    const int grp = (int)(item - (unsigned)q * (unsigned)n_groups);
+    const double4 *pm4q = fb.pm4q + (size_t)q * n;
+    const double4 *node_aq = fb.node_aq + (size_t)q * cap;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
     const int s = g0 + lane;
@@ -367,9 +392,9 @@ __global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, Traversa
             const int sp = meta.y + k;
             if (sp == s) continue;
             if (ws.pm4[sp].w == 0.0) continue;
-            const double4 q = pm4q[sp];
-            const double dx = __dsub_rn(q.x, tq.x), dy = __dsub_rn(q.y, tq.y), dz = __dsub_rn(q.z, tq.z);
-            singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
+            const double4 u = pm4q[sp];
+            const double dx = __dsub_rn(u.x, tq.x), dy = __dsub_rn(u.y, tq.y), dz = __dsub_rn(u.z, tq.z);
+            singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), u.w, g, soft2, ax, ay, az);
           }
           resume = meta.x;
         } else if (a.w == 0.0) {
@@ -390,10 +415,10 @@ __global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, Traversa
       node = __reduce_min_sync(kFull, resume);
     }
     if (valid) {
-      const uint32_t ti = ws.idx[s];
-      out.ax[ti] = ax;
-      out.ay[ti] = ay;
-      out.az[ti] = az;
+      const size_t ti = (size_t)q * n + ws.idx[s];
+      fb.ax[ti] = ax;
+      fb.ay[ti] = ay;
+      fb.az[ti] = az;
     }
   }
   if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
@@ -475,7 +500,7 @@ cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const 
   if (e != cudaSuccess) return e;
   const int grid = grid_of_ws(ws, 8);
   adj_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
-  adj_topology_kernel<<<grid, kBlock, 0, s>>>(ws, ab.pparent, ab.prange);
+  adj_topology_kernel<<<grid, kBlock, 0, s>>>(ws, ab.pparent, ab.prange, nullptr);
   adjoint_walk_kernel<<<grid_of_ws(ws, 8), 256, 0, s>>>(ws, p, ab);
   adj_node_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
   adj_leaf_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
@@ -483,20 +508,14 @@ cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_frozen_topology(Workspace &ws, int *pparent, int2 *prange, cudaStream_t s) {
-  adj_topology_kernel<<<grid_of_ws(ws, 8), kBlock, 0, s>>>(ws, pparent, prange);
-  count_launches(1);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_frozen_force(Workspace &ws, const TraversalParams &p, const FrozenCopy &c,
-                                const int2 *prange, double4 *pm4q, double4 *node_aq, cudaStream_t s) {
+cudaError_t launch_frozen_force(Workspace &ws, const TraversalParams &p, const FrozenBatch &fb, cudaStream_t s) {
   const int grid = grid_of_ws(ws, 8);
   adj_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
-  frozen_gather_kernel<<<grid, kBlock, 0, s>>>(ws, c, pm4q);
-  frozen_mass_kernel<<<grid, kBlock, 0, s>>>(ws, prange, pm4q, node_aq);
-  frozen_walk_kernel<<<grid, 256, 0, s>>>(ws, p, pm4q, node_aq, c);
-  count_launches(4);
+  adj_topology_kernel<<<grid, kBlock, 0, s>>>(ws, fb.pparent, fb.prange, fb.pre_of);
+  frozen_gather_kernel<<<grid, kBlock, 0, s>>>(ws, fb);
+  for (int level = ws.max_level; level >= 0; --level) frozen_level_kernel<<<grid, kBlock, 0, s>>>(ws, fb, level);
+  frozen_walk_kernel<<<grid, 256, 0, s>>>(ws, p, fb);
+  count_launches(5 + ws.max_level);
   return cudaGetLastError();
 }
 

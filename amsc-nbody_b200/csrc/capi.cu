@@ -1289,62 +1289,47 @@ int nbb_frozen_rollout(const nbb_config *cfg, size_t n, const double *mass, cons
   if (st) return st;
   Workspace &ws = sim->ws;
   cudaStream_t s = sim->stream;
-  const size_t bytes = n * sizeof(double);
+  const size_t bytes = n * sizeof(double), qn = copies * n, qcap = copies * (size_t)ws.cap_nodes;
   Allocation al;
-  std::vector<FrozenCopy> cp(copies);
-  double4 *pm4q = nullptr, *node_aq = nullptr;
-  int *pparent = nullptr;
-  int2 *prange = nullptr;
-  cudaError_t e = al.get(pm4q, n);
-  if (e == cudaSuccess) e = al.get(node_aq, (size_t)ws.cap_nodes);
-  if (e == cudaSuccess) e = al.get(pparent, (size_t)ws.cap_nodes);
-  if (e == cudaSuccess) e = al.get(prange, (size_t)ws.cap_nodes);
+  FrozenBatch fb;
+  fb.copies = (int)copies;
+  double **fields[10] = {&fb.m, &fb.x, &fb.y, &fb.z, &fb.vx, &fb.vy, &fb.vz, &fb.ax, &fb.ay, &fb.az};
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = al.get(*fields[k], qn);
+  if (e == cudaSuccess) e = al.get(fb.pm4q, qn);
+  if (e == cudaSuccess) e = al.get(fb.aq_oct, qcap);
+  if (e == cudaSuccess) e = al.get(fb.node_aq, qcap);
+  if (e == cudaSuccess) e = al.get(fb.pre_of, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(fb.pparent, (size_t)ws.cap_nodes);
+  if (e == cudaSuccess) e = al.get(fb.prange, (size_t)ws.cap_nodes);
   const double *src[7] = {cmass, cx, cy, cz, cvx, cvy, cvz};
-  for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
-    double *arr[10];
-    for (int k = 0; k < 10 && e == cudaSuccess; ++k) e = al.get(arr[k], n);
-    if (e != cudaSuccess) break;
-    FrozenCopy &c = cp[q];
-    c.m = arr[0]; c.x = arr[1]; c.y = arr[2]; c.z = arr[3];
-    c.vx = arr[4]; c.vy = arr[5]; c.vz = arr[6];
-    c.ax = arr[7]; c.ay = arr[8]; c.az = arr[9];
-    for (int k = 0; k < 7 && e == cudaSuccess; ++k) {
-      if (src[k])
-        e = cudaMemcpyAsync(arr[k], src[k] + q * n, bytes, copy_kind(on_device, true), s);
-      else
-        e = cudaMemcpyAsync(arr[k], ws.m, bytes, cudaMemcpyDeviceToDevice, s);
+  for (int k = 0; k < 7 && e == cudaSuccess; ++k) {
+    if (src[k]) {
+      e = cudaMemcpyAsync(*fields[k], src[k], copies * bytes, copy_kind(on_device, true), s);
+    } else {
+      for (size_t q = 0; q < copies && e == cudaSuccess; ++q)
+        e = cudaMemcpyAsync(*fields[k] + q * n, ws.m, bytes, cudaMemcpyDeviceToDevice, s);
     }
   }
   if (e != cudaSuccess) return cuda_fail(e, "frozen rollout setup");
   const TraversalParams tp = traversal_params(sim, 0);
   const double dt = c2.time_step;
-  e = launch_frozen_topology(ws, pparent, prange, s);
-  for (size_t q = 0; q < copies && e == cudaSuccess; ++q)
-    e = launch_frozen_force(ws, tp, cp[q], prange, pm4q, node_aq, s);
+  e = launch_frozen_force(ws, tp, fb, s);
   for (uint64_t k = 0; k < steps && e == cudaSuccess; ++k) {
-    for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
-      const FrozenCopy &c = cp[q];
-      e = launch_kick_drift(c.x, c.y, c.z, c.vx, c.vy, c.vz, c.ax, c.ay, c.az, n, dt, s);
-    }
+    e = launch_kick_drift(fb.x, fb.y, fb.z, fb.vx, fb.vy, fb.vz, fb.ax, fb.ay, fb.az, qn, dt, s);
     if (e == cudaSuccess) e = enqueue_rebuild_force(ws, traversal_params(sim, 1), dt, 1, s);
-    if (e == cudaSuccess) e = launch_frozen_topology(ws, pparent, prange, s);
-    for (size_t q = 0; q < copies && e == cudaSuccess; ++q) {
-      const FrozenCopy &c = cp[q];
-      e = launch_frozen_force(ws, tp, c, prange, pm4q, node_aq, s);
-      if (e == cudaSuccess) e = launch_kick(c.vx, c.vy, c.vz, c.ax, c.ay, c.az, n, dt, s);
-    }
+    if (e == cudaSuccess) e = launch_frozen_force(ws, tp, fb, s);
+    if (e == cudaSuccess) e = launch_kick(fb.vx, fb.vy, fb.vz, fb.ax, fb.ay, fb.az, qn, dt, s);
   }
   if (e != cudaSuccess) return cuda_fail(e, "frozen rollout");
   st = check_device(ws, s);
   if (st) return st;
   double *outs[6] = {ox, oy, oz, ovx, ovy, ovz};
-  for (size_t q = 0; q < copies; ++q) {
-    const double *from[6] = {cp[q].x, cp[q].y, cp[q].z, cp[q].vx, cp[q].vy, cp[q].vz};
-    for (int k = 0; k < 6; ++k)
-      if (outs[k])
-        NBB_CUDA(cudaMemcpyAsync(outs[k] + q * n, from[k], bytes, copy_kind(on_device, false), s),
-                 "copy frozen rollout state");
-  }
+  const double *from[6] = {fb.x, fb.y, fb.z, fb.vx, fb.vy, fb.vz};
+  for (int k = 0; k < 6; ++k)
+    if (outs[k])
+      NBB_CUDA(cudaMemcpyAsync(outs[k], from[k], copies * bytes, copy_kind(on_device, false), s),
+               "copy frozen rollout state");
   NBB_CUDA(cudaStreamSynchronize(s), "frozen rollout synchronisation");
   return ok();
 }

@@ -298,22 +298,27 @@ struct AdjointBuffers {
   int *pparent = nullptr;     // per preorder node
   int2 *prange = nullptr;     // per preorder node
 };
-// A perturbed copy of the particles (original order).
-struct FrozenCopy {
+// Perturbed copies of the particles: field arrays of copies * n values,
+// copy q at offset q * n (original order), plus per-copy scratch.
+struct FrozenBatch {
+  int copies = 0;
   double *m = nullptr, *x = nullptr, *y = nullptr, *z = nullptr;
   double *vx = nullptr, *vy = nullptr, *vz = nullptr;
   double *ax = nullptr, *ay = nullptr, *az = nullptr;
+  double4 *pm4q = nullptr;     // copies * n, Morton order of the unperturbed tree
+  double4 *aq_oct = nullptr;   // copies * cap_nodes, by octree id
+  double4 *node_aq = nullptr;  // copies * cap_nodes, by preorder id
+  int *pre_of = nullptr;       // cap_nodes
+  int *pparent = nullptr;      // cap_nodes
+  int2 *prange = nullptr;      // cap_nodes
 };
 // VJP of the plain FP64 force on the current tree (built from the positions
 // in the workspace): accumulates into ab.gx / gy / gz / gm.
 cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,
                                  cudaStream_t s);
-// Preorder parents and particle ranges of the current tree.
-cudaError_t launch_frozen_topology(Workspace &ws, int *pparent, int2 *prange, cudaStream_t s);
-// Force on a perturbed copy with the current tree's structure (accelerations
-// into c.ax / ay / az).
-cudaError_t launch_frozen_force(Workspace &ws, const TraversalParams &p, const FrozenCopy &c,
-                                const int2 *prange, double4 *pm4q, double4 *node_aq, cudaStream_t s);
+// Forces on every perturbed copy with the current tree's structure
+// (accelerations into fb.ax / ay / az).
+cudaError_t launch_frozen_force(Workspace &ws, const TraversalParams &p, const FrozenBatch &fb, cudaStream_t s);
 // Adjoint of the FP64 direct sum (accumulating).
 cudaError_t launch_direct_vjp(size_t n, const double *m, const double *x, const double *y, const double *z,
                               const double *gvx, const double *gvy, const double *gvz, double coef, double g,

@@ -11,6 +11,8 @@ error against FP64 direct summation on 4096 seeded targets is reported
 <= 1e-3.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nbb|reference]
+  python bench.py --workload disk|blobs|ensemble|adjoint   (secondary workloads of
+                                                             nbb.workloads, one GPU)
 
 With N > 1 (launched by torch.distributed.run) every rank steps an
 independent replica on its own GPU ("replicas only": the path has no
@@ -331,8 +333,15 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--workload", choices=["plummer", "disk", "blobs", "ensemble", "adjoint"],
+                    default="plummer")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload != "plummer":
+        from nbb import workloads
+
+        print(json.dumps(workloads.WORKLOADS[args.workload]()), flush=True)
+        return
     rank, world, local = dist_setup()
     try:
         if args.impl == "reference":
