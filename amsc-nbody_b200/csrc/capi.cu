@@ -311,7 +311,7 @@ int check_device(const Workspace &ws, cudaStream_t s) {
 // the rebuild; kick: second half kick fused into the traversal).
 cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, double dt, int kd,
                                   cudaStream_t s) {
-  ws.group_max = (tp.group_mode && tp.group_size > 32) ? 64 : 32;
+  ws.group_max = (tp.group_mode && tp.group_size > 32) ? (tp.group_size > 64 ? 128 : 64) : 32;
   cudaError_t e = launch_step_reset(ws, s);
   if (e == cudaSuccess) e = launch_kd_bbox(ws, dt, kd, s);
   if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
@@ -428,8 +428,8 @@ static int validate_config(const nbb_config *c) {
     return fail(NBB_ERR_INVALID_ARGUMENT, "Gravitational constant must be finite and positive");
   if (c->precision != NBB_PRECISION_FP64 && c->precision != NBB_PRECISION_MIXED)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown traversal precision");
-  if (c->group_size != 0 && c->group_size != 32 && c->group_size != 64)
-    return fail(NBB_ERR_INVALID_ARGUMENT, "group_size must be 0 (tuned), 32 or 64");
+  if (c->group_size != 0 && c->group_size != 32 && c->group_size != 64 && c->group_size != 128)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "group_size must be 0 (tuned), 32, 64 or 128");
   return NBB_OK;
 }
 
@@ -548,7 +548,7 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
 
 // Group-size autotuner of the mixed walk: on the tree of the first force
 // evaluation, time the traversal (CUDA events, best of two) for each
-// candidate warp group size (32 targets = one per lane, 64 = two per lane)
+// candidate warp group size (32, 64 or 128 targets: 1, 2 or 4 per lane)
 // and keep the fastest.  The choice is cached per process for the particle
 // count's power-of-two bucket, so every simulation of that size in the
 // process uses the same size; pinning nbb_config.group_size skips tuning.
@@ -572,11 +572,11 @@ static int autotune_group_size(nbb_sim *sim) {
     cudaEvent_t e0, e1;
     NBB_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
     NBB_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
-    const int candidates[2] = {32, 64};
+    const int candidates[3] = {32, 64, 128};
     float best = 1e30f;
     int best_size = 32;
     cudaError_t e = cudaSuccess;
-    for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
       TraversalParams tp = traversal_params(sim, 0);
       tp.group_size = candidates[c];
       ws.group_max = candidates[c];
@@ -603,7 +603,7 @@ static int autotune_group_size(nbb_sim *sim) {
   }
   // the initial acceleration comes from the chosen group size
   TraversalParams tp = traversal_params(sim, 0);
-  ws.group_max = tp.group_size > 32 ? 64 : 32;
+  ws.group_max = tp.group_size;
   NBB_CUDA(launch_retarget(ws, sim->stream), "retarget");
   NBB_CUDA(launch_traversal(ws, tp, sim->stream), "traversal");
   return check_device(ws, sim->stream);

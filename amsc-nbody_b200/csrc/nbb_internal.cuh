@@ -59,7 +59,7 @@ constexpr int kSortPasses = 4;     // 8-bit digits over a single system's 30-bit
 constexpr int kMaxSortPasses = 5;  // ensemble keys: up to 9 system bits + 30 Morton bits
 
 // Largest target group supported (two targets per lane of a warp).
-constexpr int kGroupMaxLimit = 64;
+constexpr int kGroupMaxLimit = 128;
 // Largest ensemble: 3 octree levels of system id.
 constexpr int kMaxSystems = 512;
 
@@ -80,8 +80,8 @@ struct Workspace {
   int cap_nodes = 0;    // octree node capacity (sum over levels of min(8^L, n))
   int num_sms = 0;
   int fp64_grid = 0;    // persistent traversal grids (blocks)
-  int mixed_grid[2][2] = {{0, 0}, {0, 0}};  // [track source][targets per lane - 1]
-  int group_max = 32;   // largest octree target group (32 x targets per lane)
+  int mixed_grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // [track source][1, 2 or 4 targets per lane]
+  int group_max = 32;   // largest octree target group: 32, 64 or 128 (32 x target slots per lane)
 
   // key layout: an ensemble's system id sits above the 30 Morton bits and
   // adds sys_levels octree levels above the system roots

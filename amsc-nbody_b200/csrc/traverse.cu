@@ -140,6 +140,11 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
 #ifndef NBB_MIXED_MINBLOCKS
 #define NBB_MIXED_MINBLOCKS 12
 #endif
+// resident blocks per SM for the four-targets-per-lane instance (more
+// registers per thread for the targets' sums)
+#ifndef NBB_MIXED_MINBLOCKS4
+#define NBB_MIXED_MINBLOCKS4 8
+#endif
 constexpr int kMixedWarps = NBB_MIXED_WARPS;
 constexpr int kStackCap = 512;
 constexpr int kListCap = 96;
@@ -151,9 +156,20 @@ struct MixedShared {
   int src[kMixedWarps][kTrackSource ? kListCap : 1];
 };
 
+// Hardware approximate reciprocal square root (MUFU), subnormal inputs and
+// results flushed to zero: r^2 + eps^2 of a force evaluation is never
+// subnormal where it matters, and the flush saves the range fix-up that
+// rsqrtf adds around the same instruction.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Evaluate `count` list entries for this lane's kTPL targets: FP32 offsets,
-// rsqrtf plus one Newton step, plain FP32 partial sums over the batch, then
-// one Kahan-compensated addition of each batch partial into its running sum.
+// approximate rsqrt plus one Newton step, plain FP32 partial sums over the
+// batch, then one Kahan-compensated addition of each batch partial into its
+// running sum.
 //
 // With positive softening a target's own entry (a leaf particle equal to the
 // target) has offset exactly (0, 0, 0) -- both offsets are rounded from the
@@ -175,7 +191,7 @@ __device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, i
     for (int q = 0; q < kTPL; ++q) {
       const float dx = e.x - tx[q], dy = e.y - ty[q], dz = e.z - tz[q];
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-      float r = rsqrtf(r2);
+      float r = rsqrt_approx(r2);
       r = r * fmaf(-0.5f * r2, r * r, 1.5f);
       float f = e.w * (r * r * r);
       if (kTrackSource) {
@@ -209,16 +225,35 @@ struct LaneTargets {
   bool singular = false;
 };
 
+// Evaluate `count` entries for the first nq (warp-uniform) of the lane's
+// kTPL target slots: a group of g targets fills ceil(g / 32) slots, and the
+// empty ones cost nothing (the branch is taken once per batch, outside the
+// entry loop).
+template <bool kTrackSource, int kTPL>
+__device__ __forceinline__ bool eval_slots(const float4 *list, const int *src, int count, int nq,
+                                           LaneTargets<kTPL> &t, float eps2) {
+  if (kTPL >= 4 && nq >= 4)
+    return eval_batch<kTrackSource, (kTPL >= 4 ? 4 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+                                                         t.comp);
+  if (kTPL >= 3 && nq == 3)
+    return eval_batch<kTrackSource, (kTPL >= 3 ? 3 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+                                                         t.comp);
+  if (kTPL >= 2 && nq == 2)
+    return eval_batch<kTrackSource, (kTPL >= 2 ? 2 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+                                                         t.comp);
+  return eval_batch<kTrackSource, 1>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum, t.comp);
+}
+
 // Evaluate full batches of 32 from the front of the list, shifting the
 // remainder down, until fewer than 32 entries are left.
 template <bool kTrackSource, int kTPL>
 __device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, LaneTargets<kTPL> &lt_,
-                                           float eps2) {
+                                           float eps2, int nq) {
   const int lane = threadIdx.x & 31;
   int done = 0;
   while (ls - done >= 32) {
-    const bool sg = eval_batch<kTrackSource, kTPL>(list + done, src + (kTrackSource ? done : 0), 32, lt_.s,
-                                                   lt_.tx, lt_.ty, lt_.tz, eps2, lt_.sum, lt_.comp);
+    const bool sg = eval_slots<kTrackSource, kTPL>(list + done, src + (kTrackSource ? done : 0), 32, nq, lt_,
+                                                   eps2);
 #pragma unroll
     for (int q = 0; q < kTPL; ++q)
       if (lt_.valid[q]) {
@@ -252,8 +287,8 @@ __device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, Lane
 // group centre (formed in FP64, then rounded) and are evaluated by all lanes
 // in batches of 32.
 template <bool kTrackSource, int kTPL>
-__global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) traverse_mixed_kernel(Workspace ws,
-                                                                                            TraversalParams p) {
+__global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : NBB_MIXED_MINBLOCKS)
+    traverse_mixed_kernel(Workspace ws, TraversalParams p) {
   __shared__ MixedShared<kTrackSource> sh;
   DevScalars *sc = ws.sc;
   if (sc->error) return;
@@ -277,6 +312,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
     if (grp >= n_groups) break;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32 * kTPL;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32 * kTPL, n);
+    const int nq = min(kTPL, max(1, (g1 - g0 + 31) >> 5));  // occupied target slots
     LaneTargets<kTPL> T;
     double4 tp[kTPL];
     double lo[3], hi[3];
@@ -407,10 +443,10 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
         }
         ls += ltotal;
         __syncwarp();
-        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
+        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
       } else {
         __syncwarp();
-        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
+        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
         unsigned lm = __ballot_sync(kFull, cat == 2);
         while (lm) {
           const int l = __ffs(lm) - 1;
@@ -426,13 +462,13 @@ __global__ void __launch_bounds__(kMixedWarps * 32, NBB_MIXED_MINBLOCKS) travers
             }
             ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
             __syncwarp();
-            flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2);
+            flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
           }
         }
       }
     }
     if (ls > 0) {
-      const bool sg = eval_batch<kTrackSource, kTPL>(list, src, ls, T.s, T.tx, T.ty, T.tz, eps2, T.sum, T.comp);
+      const bool sg = eval_slots<kTrackSource, kTPL>(list, src, ls, nq, T, eps2);
 #pragma unroll
       for (int q = 0; q < kTPL; ++q)
         if (T.valid[q]) {
@@ -744,23 +780,24 @@ cudaError_t configure_traversal(Workspace &ws) {
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 1>, kMixedWarps * 32, sms, ws.mixed_grid[1][0]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 2>, kMixedWarps * 32, sms, ws.mixed_grid[0][1]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 2>, kMixedWarps * 32, sms, ws.mixed_grid[1][1]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 4>, kMixedWarps * 32, sms, ws.mixed_grid[0][2]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 4>, kMixedWarps * 32, sms, ws.mixed_grid[1][2]);
   return e;
 }
 
 cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p, cudaStream_t s) {
-  const int tpl = (p.group_mode && p.group_size > 32) ? 2 : 1;
+  // target slots per lane: 1, 2 or 4 for groups of at most 32, 64 or 128
+  const int slot = !p.group_mode ? 0 : (p.group_size > 64 ? 2 : (p.group_size > 32 ? 1 : 0));
   const int track = p.soft > 0.0 ? 0 : 1;
-  const int grid = ws.mixed_grid[track][tpl - 1] > 0 ? ws.mixed_grid[track][tpl - 1] : 148;
+  const int grid = ws.mixed_grid[track][slot] > 0 ? ws.mixed_grid[track][slot] : 148;
   if (p.precision == 0)
     traverse_fp64_kernel<<<ws.fp64_grid > 0 ? ws.fp64_grid : 148, 256, 0, s>>>(ws, p);
-  else if (!track && tpl == 1)
-    traverse_mixed_kernel<false, 1><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
-  else if (track && tpl == 1)
-    traverse_mixed_kernel<true, 1><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
-  else if (!track)
-    traverse_mixed_kernel<false, 2><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+  else if (slot == 0)
+    (track ? traverse_mixed_kernel<true, 1> : traverse_mixed_kernel<false, 1>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+  else if (slot == 1)
+    (track ? traverse_mixed_kernel<true, 2> : traverse_mixed_kernel<false, 2>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
   else
-    traverse_mixed_kernel<true, 2><<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+    (track ? traverse_mixed_kernel<true, 4> : traverse_mixed_kernel<false, 4>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
   count_launches(1);
   return cudaGetLastError();
 }

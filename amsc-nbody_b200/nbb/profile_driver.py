@@ -20,10 +20,12 @@ def main():
     ap.add_argument("--n", type=int, default=1 << 20)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--group-size", type=int, default=0, help="mixed walk group size (0 = tuned)")
     args = ap.parse_args()
     prec = nbb.PRECISION_MIXED if args.precision == "mixed" else nbb.PRECISION_FP64
     p = ics.plummer(args.n, seed=0)
-    sim = nbb.Simulation(p, nbb.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec))
+    sim = nbb.Simulation(p, nbb.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec,
+                                                 group_size=args.group_size))
     sim.initialize()
     sim.run(args.steps)
     stages, st = sim.profile()

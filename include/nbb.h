@@ -60,7 +60,7 @@ typedef struct {
   double softening;
   double gravitational_constant;
   int precision;  /* nbb_precision */
-  int group_size; /* MIXED: targets per warp group, 16/32/64; 0 = tuned */
+  int group_size; /* MIXED: targets per warp group, 32/64/128; 0 = tuned */
   int use_graph;  /* capture each step into a CUDA graph (default 1) */
   int device;     /* CUDA device ordinal (default 0) */
 } nbb_config;
@@ -141,7 +141,7 @@ typedef struct {
   int n_octree_nodes;   /* M */
   int64_t interactions; /* monopole + leaf-pair interactions evaluated */
   int64_t mac_tests;    /* acceptance tests evaluated */
-  int group_size;       /* MIXED: warp target group size in use (32 or 64) */
+  int group_size;       /* MIXED: warp target group size in use (32, 64 or 128) */
 } nbb_stats;
 int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats);
 

@@ -377,9 +377,9 @@ def test_mixed_force_error(nbb_mod, recipe, n, theta, soft):
         assert rms_mixed <= MIXED_RMS_BOUND, rms_mixed
 
 
-@pytest.mark.parametrize("group_size", [32, 64])
+@pytest.mark.parametrize("group_size", [32, 64, 128])
 def test_mixed_group_sizes(nbb_mod, group_size):
-    """Both warp group sizes (one or two targets per lane) stay within the
+    """Every warp group size (one, two or four targets per lane) stays within the
     headline bound and match each other to the Barnes-Hut error level."""
     from nbb import ics
 
@@ -407,7 +407,7 @@ def test_mixed_autotuned_group_size(nbb_mod):
                                                              precision=nbb_mod.PRECISION_MIXED))
         sim.initialize()
         sizes.append(sim.stats().group_size)
-    assert sizes[0] in (32, 64) and sizes[0] == sizes[1]  # cached per process and size
+    assert sizes[0] in (32, 64, 128) and sizes[0] == sizes[1]  # cached per process and size
     with pytest.raises(nbb_mod.InvalidArgument):
         nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, group_size=48))
 
