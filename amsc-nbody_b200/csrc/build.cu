@@ -15,7 +15,10 @@
 //   octree_clear_kernel   octree_builder.cu:476-509 (initialisation)
 //   materialize_kernel    octree_builder.cu:275-412
 //   node_init_kernel      octree_geometry.cu:56-102 + octree_physics.cu:236-326
-//   propagate_kernel      octree_physics.cu:328-417 (+ subtree sizes)
+//   level_bin_kernel      octree nodes binned by level
+//   propagate_level_kernel octree_physics.cu:328-417 (+ subtree sizes), one
+//                         level per launch, deepest first
+//   pre_level_kernel      preorder indices, one level per launch, root first
 //   layout_kernel         traversal records in depth-first preorder
 //
 // No kernel synchronises with the host: data-dependent sizes (G, M) live in
@@ -34,6 +37,17 @@ constexpr int kBlock = 256;
 
 inline int grid_for(const Workspace &ws, int per_sm = 8) {
   return ws.num_sms > 0 ? ws.num_sms * per_sm : 1184;
+}
+
+// Blocks for one octree level: enough for the most nodes a level can hold
+// (min(8^L, n)), at most grid_for().
+inline int level_grid(const Workspace &ws, int level) {
+  long long width = 1;
+  for (int l = 0; l < level && width < (1ll << 40); ++l) width *= 8;
+  const long long nodes = width < ws.n ? width : ws.n;
+  const long long blocks = (nodes + kBlock - 1) / kBlock;
+  const int cap = grid_for(ws, 8);
+  return blocks < 1 ? 1 : (blocks > cap ? cap : (int)blocks);
 }
 
 // ------------------------------------------------------------- reset ----
@@ -60,6 +74,7 @@ __global__ void reset_scalars_kernel(DevScalars *sc) {
     sc->stack_overflow = 0;
     sc->interactions = 0;
     sc->mac_tests = 0;
+    for (int l = 0; l < kMaxLevels; ++l) sc->level_count[l] = 0;
   }
 }
 
@@ -288,15 +303,26 @@ __global__ void __launch_bounds__(kBlock) encode_kernel(Workspace ws) {
   if (threadIdx.x == 0) s_last = (atomicAdd(&sc->ticket_encode, 1u) == gridDim.x - 1);
   __syncthreads();
   if (s_last) {
+    // digit counts -> exclusive digit offsets, one thread per digit (the
+    // counts were added at L2 by every block before its ticket)
     __threadfence();
-    if (threadIdx.x < passes) {
-      uint32_t *h = ws.digit_hist + threadIdx.x * 256;
-      uint32_t run = 0;
-      for (int d = 0; d < 256; ++d) {
-        const uint32_t c = atomicAdd(&h[d], 0u);
-        h[d] = run;
-        run += c;
+    static_assert(kBlock == 256, "one thread per digit");
+    __shared__ uint32_t warp_tot[kBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int p = 0; p < passes; ++p) {
+      uint32_t *h = ws.digit_hist + p * 256;
+      const uint32_t c = __ldcg(h + threadIdx.x);
+      uint32_t inc = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
       }
+      if (lane == 31) warp_tot[warp] = inc;
+      __syncthreads();
+      uint32_t base = 0;
+      for (int w = 0; w < warp; ++w) base += warp_tot[w];
+      h[threadIdx.x] = base + inc - c;
+      __syncthreads();
     }
   }
 }
@@ -742,7 +768,6 @@ __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
     ws.oprefix[i] = 0ull;
     ws.ofirst[i] = -1;
     ws.ocount[i] = 0;
-    ws.pending[i] = 0;
     ws.child_count[i] = 0;
     ws.subtree[i] = 0;
     ws.preoff[i] = 0;
@@ -968,123 +993,182 @@ __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
   }
 }
 
-// octree_physics.cu:328-417: bottom-up propagation with per-node arrival
-// counters; the last child to arrive combines the children in octant order
-// 0..7 (deterministic).  The same thread also sums subtree sizes and assigns
-// each child its offset within the parent's depth-first preorder (children
-// visited octant 7 -> 0).  Spin-free: a thread that is not last just stops.
-__global__ void __launch_bounds__(kBlock) propagate_kernel(Workspace ws) {
+// Octree nodes binned by level: level L owns the fixed region
+// [level_base(L), level_base(L) + min(8^L, n)) of by_level (no octree level
+// holds more nodes than that), filled in any order.
+__device__ __forceinline__ int level_base(const Workspace &ws, int level) {
+  long long base = 0, width = 1;
+  for (int l = 0; l < level; ++l) {
+    base += (width < ws.n) ? width : ws.n;
+    if (width < (1ll << 40)) width *= 8;
+  }
+  return (int)base;
+}
+__device__ __forceinline__ int level_cap(const Workspace &ws, int level) {
+  long long width = 1;
+  for (int l = 0; l < level && width < (1ll << 40); ++l) width *= 8;
+  return (int)((width < ws.n) ? width : ws.n);
+}
+
+__global__ void __launch_bounds__(kBlock) level_bin_kernel(Workspace ws) {
+  __shared__ int s_cnt[kMaxLevels], s_base[kMaxLevels];
+  __shared__ int s_m;
   DevScalars *sc = ws.sc;
-  if (sc->error) return;
-  const int m = sc->n_nodes;
-  for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < m; leaf += gridDim.x * blockDim.x) {
-    if (ws.ocount[leaf] <= 0) continue;
-    if (ws.child_count[leaf] != 0) {
-      record_error(sc, kStagePhysics, 4);
-      continue;
-    }
-    int done = leaf;
-    int parent = ws.oparent[done];
-    int climbs = 0;
-    while (parent != -1) {
-      if (parent < 0 || parent >= m || ++climbs > ws.max_level + 1) {
+  if (threadIdx.x == 0) s_m = sc->error ? 0 : sc->n_nodes;
+  __syncthreads();
+  const int m = s_m;  // block-uniform trip count below
+  for (int b0 = blockIdx.x * blockDim.x; b0 < m; b0 += gridDim.x * blockDim.x) {
+    if (threadIdx.x < kMaxLevels) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int v = b0 + threadIdx.x;
+    int level = -1, slot = 0;
+    if (v < m) {
+      level = ws.olevel[v];
+      if (level < 0 || level > ws.max_level || level >= kMaxLevels) {
         record_error(sc, kStagePhysics, 5);
-        break;
-      }
-      const int required = ws.child_count[parent];
-      if (required <= 0 || required > 8) {
-        record_error(sc, kStagePhysics, 6);
-        break;
-      }
-      __threadfence();
-      const int arrived = atomicAdd(&ws.pending[parent], 1) + 1;
-      if (arrived < required) break;
-      if (arrived > required) {
-        record_error(sc, kStagePhysics, 7);
-        break;
-      }
-      __threadfence();
-      const int4 *c4 = reinterpret_cast<const int4 *>(ws.children + (size_t)parent * 8);
-      const int4 a = c4[0], b = c4[1];
-      const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-      double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-      int size = 1;
-      int nparticles = 0;
-      int firstp = INT_MAX;
-      int sub[8];
-#pragma unroll
-      for (int o = 0; o < 8; ++o) {
-        sub[o] = 0;
-        const int c = ch[o];
-        if (c <= 0 || c >= m) continue;
-        const double cm = __ldcg(ws.mass + c);
-        tm = __dadd_rn(tm, cm);
-        wx = __fma_rn(cm, __ldcg(ws.comx + c), wx);
-        wy = __fma_rn(cm, __ldcg(ws.comy + c), wy);
-        wz = __fma_rn(cm, __ldcg(ws.comz + c), wz);
-        sub[o] = __ldcg(ws.subtree + c);
-        size += sub[o];
-        nparticles += __ldcg(ws.psub + c);
-        firstp = min(firstp, __ldcg(ws.pfirst + c));
-      }
-      ws.mass[parent] = tm;
-      if (tm > 0.0) {
-        const double inv = __ddiv_rn(1.0, tm);
-        ws.comx[parent] = __dmul_rn(wx, inv);
-        ws.comy[parent] = __dmul_rn(wy, inv);
-        ws.comz[parent] = __dmul_rn(wz, inv);
+        level = -1;
       } else {
-        ws.comx[parent] = 0.0;
-        ws.comy[parent] = 0.0;
-        ws.comz[parent] = 0.0;
+        slot = atomicAdd(&s_cnt[level], 1);
       }
-      int run = 1;
-#pragma unroll
-      for (int o = 7; o >= 0; --o) {
-        if (ch[o] <= 0 || ch[o] >= m) continue;
-        ws.preoff[ch[o]] = run;
-        run += sub[o];
-      }
-      ws.subtree[parent] = size;
-      ws.psub[parent] = nparticles;
-      ws.pfirst[parent] = firstp;
-      done = parent;
-      parent = ws.oparent[done];
     }
+    __syncthreads();
+    if (threadIdx.x < kMaxLevels && s_cnt[threadIdx.x] > 0)
+      s_base[threadIdx.x] = atomicAdd(&sc->level_count[threadIdx.x], s_cnt[threadIdx.x]);
+    __syncthreads();
+    if (level >= 0) {
+      const int pos = s_base[level] + slot;
+      if (pos < level_cap(ws, level))
+        ws.by_level[level_base(ws, level) + pos] = v;
+      else
+        record_error(sc, kStagePhysics, 5);
+    }
+    __syncthreads();
+  }
+}
+
+// octree_physics.cu:328-417, one octree level per launch, deepest first:
+// every internal node of the level combines its (finished) children in
+// octant order 0..7 -- the reference's deterministic order, so mass and
+// centre of mass are bit-identical -- and also sums its subtree size,
+// particle count and first particle and assigns each child its offset
+// within the node's depth-first preorder range (children visited 7 -> 0).
+// The device scalars a level launch needs, read once per block (every
+// thread reading the same word would queue at one L2 slice).
+struct LevelScalars {
+  int m, count;
+};
+__device__ __forceinline__ LevelScalars level_scalars(const Workspace &ws, int level) {
+  __shared__ LevelScalars s;
+  if (threadIdx.x == 0) {
+    const DevScalars *sc = ws.sc;
+    s.m = sc->error ? 0 : sc->n_nodes;
+    s.count = sc->error ? 0 : min(sc->level_count[level], level_cap(ws, level));
+  }
+  __syncthreads();
+  return s;
+}
+
+__global__ void __launch_bounds__(kBlock) propagate_level_kernel(Workspace ws, int level) {
+  DevScalars *sc = ws.sc;
+  const LevelScalars ls = level_scalars(ws, level);
+  const int m = ls.m, count = ls.count;
+  const int base = level_base(ws, level);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int node = ws.by_level[base + i];
+    if (node < 0 || node >= m || ws.child_count[node] == 0) continue;  // leaves: node_init_kernel
+    const int4 *c4 = reinterpret_cast<const int4 *>(ws.children + (size_t)node * 8);
+    const int4 a = c4[0], b = c4[1];
+    const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    int size = 1, nparticles = 0, firstp = INT_MAX;
+    int sub[8];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+      sub[o] = 0;
+      const int c = ch[o];
+      if (c <= 0 || c >= m) continue;
+      if (ws.olevel[c] <= level) {
+        record_error(sc, kStagePhysics, 5);
+        continue;
+      }
+      const double cm = ws.mass[c];
+      tm = __dadd_rn(tm, cm);
+      wx = __fma_rn(cm, ws.comx[c], wx);
+      wy = __fma_rn(cm, ws.comy[c], wy);
+      wz = __fma_rn(cm, ws.comz[c], wz);
+      sub[o] = ws.subtree[c];
+      size += sub[o];
+      nparticles += ws.psub[c];
+      firstp = min(firstp, ws.pfirst[c]);
+    }
+    ws.mass[node] = tm;
+    if (tm > 0.0) {
+      const double inv = __ddiv_rn(1.0, tm);
+      ws.comx[node] = __dmul_rn(wx, inv);
+      ws.comy[node] = __dmul_rn(wy, inv);
+      ws.comz[node] = __dmul_rn(wz, inv);
+    } else {
+      ws.comx[node] = 0.0;
+      ws.comy[node] = 0.0;
+      ws.comz[node] = 0.0;
+    }
+    int run = 1;
+#pragma unroll
+    for (int o = 7; o >= 0; --o) {
+      if (ch[o] <= 0 || ch[o] >= m) continue;
+      ws.preoff[ch[o]] = run;
+      run += sub[o];
+    }
+    ws.subtree[node] = size;
+    ws.psub[node] = nparticles;
+    ws.pfirst[node] = firstp;
   }
 }
 
 // --------------------------------------------------------------- layout --
 
 // Traversal records in depth-first preorder with children visited octant
-// 7 -> 0 (the reference's traversal order, barnes_hut.cu:110-182): node n sits
-// at pre(n) = sum of the preorder offsets on its path to the root, its
+// 7 -> 0 (the reference's traversal order, barnes_hut.cu:110-182).  Preorder
+// indices go top-down, one octree level per launch: node n sits at
+// pre(n) = pre(parent) + its offset within the parent's range; then one
+// launch over all nodes writes the records.  Its
 // subtree ends at pre(n) + size(n) ("skip"), and its children are listed in
 // visit order.  The acceptance radius crit = side/theta + |com - centre|
 // (barnes_hut.cu:297-311) is precomputed once per node, with a +-2^-44 band
 // around crit^2 inside which the traversal falls back to the exact
 // sqrt(d^2) > crit comparison.
+__global__ void __launch_bounds__(kBlock) pre_level_kernel(Workspace ws, int level) {
+  DevScalars *sc = ws.sc;
+  const LevelScalars ls = level_scalars(ws, level);
+  const int m = ls.m, count = ls.count;
+  const int base = level_base(ws, level);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const int node = ws.by_level[base + i];
+    if (node < 0 || node >= m) continue;
+    // the parent sits at a smaller level and got its index in an earlier launch
+    int pre = 0;
+    if (node != 0) {
+      const int par = ws.oparent[node];
+      if (par < 0 || par >= m || ws.olevel[par] >= level) {
+        record_error(sc, kStageLayout, 1);
+        continue;
+      }
+      pre = ws.pre_of[par] + ws.preoff[node];
+    }
+    if (pre < 0 || pre >= m) {
+      record_error(sc, kStageLayout, 1);
+      pre = 0;
+    }
+    ws.pre_of[node] = pre;
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double theta) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int m = sc->n_nodes;
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
-    int pre = 0;
-    int v = node;
-    int guard = 0;
-    while (v != 0) {
-      pre += ws.preoff[v];
-      v = ws.oparent[v];
-      if (v < 0 || ++guard > ws.max_level + 1) {
-        record_error(sc, kStageLayout, 1);
-        break;
-      }
-    }
-    if (v != 0) continue;
-    if (pre < 0 || pre >= m) {
-      record_error(sc, kStageLayout, 1);
-      continue;
-    }
+    const int pre = ws.pre_of[node];
     const double h = ws.half[node];
     const int lvl = ws.olevel[node];
     if (lvl == ws.sys_levels) ws.root_pre[ws.oprefix[node] >> kSpatialBits] = pre;
@@ -1310,11 +1394,15 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
   materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
   node_init_kernel<<<grid, kBlock, 0, s>>>(ws);
-  propagate_kernel<<<grid, kBlock, 0, s>>>(ws);
+  level_bin_kernel<<<grid, kBlock, 0, s>>>(ws);
+  for (int level = ws.max_level; level >= 0; --level)
+    propagate_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
+  for (int level = 0; level <= ws.max_level; ++level)
+    pre_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
   layout_kernel<<<grid, kBlock, 0, s>>>(ws, theta);
   group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(9);
+  count_launches(9 + 2 * (ws.max_level + 1));
   return cudaGetLastError();
 }
 

@@ -212,7 +212,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.plevel, 2 * N); GET(ws.pcount, 2 * N); GET(ws.poffset, 2 * N);
   GET(ws.children, 8 * C);
   GET(ws.oparent, C); GET(ws.olevel, C); GET(ws.oprefix, C); GET(ws.ofirst, C); GET(ws.ocount, C);
-  GET(ws.child_count, C); GET(ws.pending, C); GET(ws.subtree, C); GET(ws.preoff, C);
+  GET(ws.child_count, C); GET(ws.pre_of, C); GET(ws.by_level, C); GET(ws.subtree, C); GET(ws.preoff, C);
   GET(ws.psub, C); GET(ws.pfirst, C);
   GET(ws.tflag, N); GET(ws.tstart, N);
   GET(ws.cx, C); GET(ws.cy, C); GET(ws.cz, C); GET(ws.half, C);

@@ -49,6 +49,7 @@ struct DevScalars {
   unsigned int stack_overflow;   // mixed traversal nodes accepted on overflow
   unsigned long long interactions;
   unsigned long long mac_tests;
+  int level_count[16];           // octree nodes per level (kMaxLevels)
 };
 
 // Sort tiling (onesweep LSD radix sort of packed (key << 32 | index)).
@@ -57,6 +58,7 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 pairs
 constexpr int kSortPasses = 4;     // 8-bit digits over a single system's 30-bit keys
 constexpr int kMaxSortPasses = 5;  // ensemble keys: up to 9 system bits + 30 Morton bits
+constexpr int kMaxLevels = 16;     // octree levels: 10 spatial + up to 3 above the system roots
 
 // Largest target group supported (two targets per lane of a warp).
 constexpr int kGroupMaxLimit = 128;
@@ -136,7 +138,8 @@ struct Workspace {
   int *children = nullptr, *oparent = nullptr, *olevel = nullptr;
   unsigned long long *oprefix = nullptr;
   int *ofirst = nullptr, *ocount = nullptr, *child_count = nullptr,
-      *pending = nullptr;
+      *pre_of = nullptr;    // preorder index by octree id
+  int *by_level = nullptr;  // octree ids binned by level (fixed region per level)
   double *cx = nullptr, *cy = nullptr, *cz = nullptr, *half = nullptr;
   double *mass = nullptr, *comx = nullptr, *comy = nullptr, *comz = nullptr;
   int *subtree = nullptr, *preoff = nullptr;
@@ -179,6 +182,15 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(
 __device__ __forceinline__ void st_release_u64(unsigned long long *p,
                                                unsigned long long v) {
   asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Arrival counter increment with acquire-release ordering at GPU scope: the
+// caller's earlier writes are visible to whoever sees the new count, and the
+// caller sees every write released by earlier arrivals.
+__device__ __forceinline__ int arrive_acq_rel(int *counter) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+  return old;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
