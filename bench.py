@@ -67,7 +67,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -303,12 +303,14 @@ def build_algorithmic_bytes(n, groups, nodes):
             + BUILD_BYTES_PER_RADIX_NODE * (2 * groups - 1) + BUILD_BYTES_PER_OCTREE_NODE * nodes)
 
 
-def profiled_traffic(kernel_file):
-    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+def profiled_traffic(kernel_file, variant=None):
+    """DRAM bytes per launch of a kernel from its committed ncu summary
+    (the line for `variant`, e.g. the warp group size, when given)."""
     path = os.path.join(ROOT, "profiles", kernel_file)
+    key = "dram_bytes_per_launch" + (f"[{variant}]" if variant is not None else "") + ":"
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
+            if line.startswith(key):
                 return int(line.split(":")[1])
     except OSError:
         pass
@@ -327,7 +329,7 @@ def load_peaks():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["nbb", "reference"], default="nbb")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
@@ -393,7 +395,7 @@ def bench_nbb(args, rank, world, local):
     sm_mhz = clocks.get("sm_max_mhz") or 1965.0
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                         "frac": achieved / peak32,
-                        "traffic": profiled_traffic("traverse_mixed_plummer_2e20.md"),
+                        "traffic": profiled_traffic("traverse_mixed_plummer_2e20.md", mixed["group_size"]),
                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                           "launch (profiles/traverse_mixed_plummer_2e20.md)",
                         "kernel": "traverse_mixed_kernel",
@@ -406,6 +408,7 @@ def bench_nbb(args, rank, world, local):
     p_ach = 20.0 * plain["interactions"] / (ptrav * 1e-3) / 1e12
     line["plain_fp64"]["roofline"] = {"bound": "fp64", "achieved": p_ach, "peak": peak64,
                                       "unit": "TFLOP/s", "frac": p_ach / peak64,
+                                      "traffic": profiled_traffic("traverse_fp64_plummer_2e20.md"),
                                       "kernel": "traverse_fp64_kernel",
                                       "interactions_per_s": plain["interactions"] / (ptrav * 1e-3)}
     peaks = load_peaks()
