@@ -1,9 +1,12 @@
 // nbody_cli.cpp -- command-line driver with the reference's interface
 // (apps/simulation/main.cpp:44-333 of sytrams/AMSC-Nbody): same options,
 // output lines and exit codes (0 success, 2 argument error with usage, 1
-// runtime failure).  The frame-streaming options of the reference belong to
-// its viewer stack, which this library does not provide; they are rejected
-// as argument errors.  Additions: --precision and --gravitational-constant.
+// runtime failure).  --stream-dir, --sample-rate and --stream-max-particles
+// write quantized frames to a spool directory as the reference does; its
+// stream server options (--cluster, --stream-bind, --stream-port,
+// --stream-server) belong to a viewer stack this library does not provide
+// and are rejected as argument errors.  Additions: --precision and
+// --gravitational-constant.
 #include <cerrno>
 #include <charconv>
 #include <chrono>
@@ -12,11 +15,14 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <string_view>
 
 #include "nbb_simulation.hpp"
+#include "nbb_streaming.hpp"
 
 namespace {
 
@@ -25,6 +31,10 @@ struct Options {
   std::size_t steps = 0;
   SimulationConfig simulation{0.0, 0.5, 1.0e-6};
   SimulationOptions extra{};
+  std::string streamDirectory;
+  double sampleRate = 60.0;
+  std::size_t maximumStreamParticles = 100000;
+  bool streamEnabled = false;
   bool showHelp = false;
   bool hasTimeStep = false;
   bool hasSteps = false;
@@ -42,6 +52,10 @@ void printUsage(std::ostream &out, const char *program) {
       << "      --softening VALUE  Non-negative softening length (default: 1e-6)\n"
       << "      --precision MODE   fp64 (reference arithmetic) or mixed (default: fp64)\n"
       << "      --gravitational-constant VALUE  G (default: 6.6743e-11)\n\n"
+      << "Frame output options:\n"
+      << "      --stream-dir DIR   Durable frame queue; also enables output\n"
+      << "      --sample-rate HZ   Maximum wall-clock sample rate (default: 60)\n"
+      << "      --stream-max-particles N  Frame sample size; 0 writes all (default: 100000)\n\n"
       << "Other options:\n"
       << "  -h, --help             Show this help and exit\n";
 }
@@ -58,6 +72,14 @@ double parseDouble(std::string_view text, std::string_view option) {
   const double v = std::strtod(s.c_str(), &end);
   if (end == s.c_str() || *end != '\0' || errno == ERANGE || !std::isfinite(v))
     throw std::invalid_argument("Invalid numeric value for " + std::string(option) + ": " + s);
+  return v;
+}
+
+std::size_t parseNonNegativeCount(std::string_view text, std::string_view option) {
+  std::size_t v = 0;
+  const auto r = std::from_chars(text.data(), text.data() + text.size(), v);
+  if (r.ec != std::errc{} || r.ptr != text.data() + text.size())
+    throw std::invalid_argument("Invalid non-negative integer for " + std::string(option) + ": " + std::string(text));
   return v;
 }
 
@@ -100,10 +122,15 @@ Options parseCommandLine(int argc, char **argv) {
       } else {
         throw std::invalid_argument("Invalid value for --precision: " + std::string(v));
       }
-    } else if (opt == "--cluster" || opt == "--stream-dir" || opt == "--sample-rate" ||
-               opt == "--stream-max-particles" || opt == "--stream-bind" || opt == "--stream-port" ||
-               opt == "--stream-server") {
-      throw std::invalid_argument("Frame streaming is not part of this build: " + std::string(opt));
+    } else if (opt == "--stream-dir") {
+      o.streamDirectory = requireValue(argc, argv, i, opt);
+      o.streamEnabled = true;
+    } else if (opt == "--sample-rate") {
+      o.sampleRate = parseDouble(requireValue(argc, argv, i, opt), opt);
+    } else if (opt == "--stream-max-particles") {
+      o.maximumStreamParticles = parseNonNegativeCount(requireValue(argc, argv, i, opt), opt);
+    } else if (opt == "--cluster" || opt == "--stream-bind" || opt == "--stream-port" || opt == "--stream-server") {
+      throw std::invalid_argument("The stream server is not part of this build: " + std::string(opt));
     } else {
       throw std::invalid_argument("Unknown option: " + std::string(opt));
     }
@@ -114,6 +141,8 @@ Options parseCommandLine(int argc, char **argv) {
   if (o.simulation.timeStep <= 0.0) throw std::invalid_argument("--time-step must be positive");
   if (o.simulation.theta < 0.0) throw std::invalid_argument("--theta must be non-negative");
   if (o.simulation.softening < 0.0) throw std::invalid_argument("--softening must be non-negative");
+  if (o.sampleRate <= 0.0) throw std::invalid_argument("--sample-rate must be positive");
+  if (o.streamEnabled && o.streamDirectory.empty()) throw std::invalid_argument("--stream-dir must not be empty");
   return o;
 }
 
@@ -128,14 +157,38 @@ int main(int argc, char **argv) {
     }
     std::ifstream input(options.inputPath, std::ios::binary);
     if (!input.is_open()) throw std::runtime_error("Could not open particle input file: " + options.inputPath);
+    std::unique_ptr<nbody::streaming::FrameSpool> spool;
+    std::unique_ptr<nbody::streaming::FrameSampler> sampler;
+    if (options.streamEnabled) {
+      spool = std::make_unique<nbody::streaming::FrameSpool>(options.streamDirectory);
+      sampler = std::make_unique<nbody::streaming::FrameSampler>(options.sampleRate);
+    }
     Particles particles(input);
     const std::size_t count = particles.size();
     Simulation simulation(std::move(particles), options.simulation, options.extra);
+    std::unique_ptr<nbody::streaming::DeviceFrameWriter> writer;
+    if (spool) writer = std::make_unique<nbody::streaming::DeviceFrameWriter>(simulation, options.maximumStreamParticles);
     std::cout << "Loaded " << count << " particles from " << options.inputPath << '\n';
     const auto initStart = std::chrono::steady_clock::now();
     simulation.initialize();
     const auto initEnd = std::chrono::steady_clock::now();
-    for (std::size_t s = 0; s < options.steps; ++s) simulation.step();
+    std::size_t framesWritten = 0;
+    std::size_t lastCaptured = std::numeric_limits<std::size_t>::max();
+    auto capture = [&](bool force) {
+      if (!sampler) return;
+      const std::chrono::duration<double> elapsed = std::chrono::steady_clock::now() - initEnd;
+      if (!force && !sampler->isDue(elapsed.count())) return;
+      (void)writer->write(*spool, sampler->takeSequence());
+      ++framesWritten;
+      lastCaptured = simulation.stepNumber();
+    };
+    capture(false);
+    for (std::size_t s = 0; s < options.steps; ++s) {
+      simulation.step();
+      capture(false);
+    }
+    if (sampler && lastCaptured != simulation.stepNumber()) capture(true);
+    if (spool) (void)spool->markComplete();
     const auto evolEnd = std::chrono::steady_clock::now();
     const std::chrono::duration<double> initElapsed = initEnd - initStart;
     const std::chrono::duration<double> evolElapsed = evolEnd - initEnd;
@@ -148,6 +201,11 @@ int main(int argc, char **argv) {
               << "  average step time: " << 1000.0 * evolElapsed.count() / static_cast<double>(options.steps)
               << " ms\n"
               << "  total wall time: " << total.count() << " seconds\n";
+    if (spool) {
+      std::cout << "  frames written: " << framesWritten << '\n'
+                << "  particles per frame: " << writer->sampleParticleCount() << " of " << count << '\n'
+                << "  frame spool: " << spool->directory() << '\n';
+    }
     return 0;
   } catch (const std::invalid_argument &error) {
     std::cerr << "Argument error: " << error.what() << "\n\n";

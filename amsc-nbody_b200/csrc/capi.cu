@@ -355,6 +355,14 @@ struct RolloutRecord {
   int2 *prange = nullptr;
 };
 
+// Device buffers of frame capture, taken at the first capture.
+struct FrameBuffers {
+  Allocation al;
+  size_t bytes = 0;
+  unsigned char *frame = nullptr;
+  FrameScalars *scalars = nullptr;
+};
+
 struct nbb_sim {
   nbb_config cfg{};
   Workspace ws{};
@@ -370,6 +378,7 @@ struct nbb_sim {
   int tuned_group_size = 0;
   double min_softening = 0.0;  // ensembles: smallest per-system softening
   std::unique_ptr<RolloutRecord> rollout;
+  std::unique_ptr<FrameBuffers> frames;
 };
 
 extern "C" {
@@ -1406,6 +1415,77 @@ int nbb_direct_rollout_adjoint(const nbb_config *cfg, size_t n, const double *ma
     if (outs[k]) e = cudaMemcpyAsync(outs[k], from[k], bytes, copy_kind(on_device, false), s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "direct adjoint");
+  return ok();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ frame capture ----
+
+namespace {
+
+size_t frame_samples(size_t n, size_t max_particles) {
+  return (max_particles == 0 || max_particles > n) ? n : max_particles;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t nbb_frame_bytes(const nbb_sim *sim, size_t max_particles) {
+  if (!sim) return 0;
+  return (size_t)kFrameHeaderBytes + 7 * frame_samples((size_t)sim->ws.n, max_particles);
+}
+
+int nbb_sim_capture_frame(nbb_sim *sim, size_t max_particles, uint64_t sequence, void *out, size_t capacity,
+                          size_t *written, int on_device) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (!out) return fail(NBB_ERR_INVALID_ARGUMENT, "null frame buffer");
+  if (sim->state == nbb_sim::State::failed) return fail(NBB_ERR_LOGIC, "Simulation is in a failed state");
+  if (!std::isfinite(sim->time) || sim->time < 0.0) return fail(NBB_ERR_INVALID_ARGUMENT, "Frame simulation time is invalid");
+  const size_t n = (size_t)sim->ws.n;
+  const size_t s = frame_samples(n, max_particles);
+  const size_t bytes = (size_t)kFrameHeaderBytes + 7 * s;
+  if (capacity < bytes) return fail(NBB_ERR_INVALID_ARGUMENT, "frame buffer is smaller than nbb_frame_bytes()");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  if (!sim->frames || sim->frames->bytes < bytes) {
+    auto fb = std::make_unique<FrameBuffers>();
+    NBB_CUDA(fb->al.get(fb->frame, bytes), "Could not allocate the quantized sampling buffer");
+    NBB_CUDA(fb->al.get(fb->scalars, 1), "Could not allocate the sampling bounds buffer");
+    fb->bytes = bytes;
+    sim->frames = std::move(fb);
+  }
+  FrameBuffers &fb = *sim->frames;
+  const Workspace &ws = sim->ws;
+  cudaStream_t st = sim->stream;
+  FrameHeaderFields h;
+  h.sequence = sequence;
+  h.step = sim->steps;
+  h.time = sim->time;
+  h.source_count = n;
+  h.sample_count = s;
+  NBB_CUDA(launch_frame_capture(ws.x, ws.y, ws.z, ws.type, n, s, fb.scalars, h, fb.frame, st),
+           "Could not launch the graphical quantization kernel");
+  FrameScalars f;
+  NBB_CUDA(cudaMemcpyAsync(&f, fb.scalars, sizeof(f), cudaMemcpyDeviceToHost, st), "Could not validate graphical samples");
+  NBB_CUDA(cudaStreamSynchronize(st), "Could not validate graphical samples");
+  if (f.nonfinite) return fail(NBB_ERR_DOMAIN, "Cannot quantize a graphical frame with non-finite positions");
+  if (f.bad_type) return fail(NBB_ERR_INVALID_ARGUMENT, "Cannot capture a frame with invalid particle types");
+  for (int a = 0; a < 3; ++a) {
+    double lo, hi;
+    const unsigned long long bl = f.lo[a], bh = f.hi[a];
+    // decode the order-preserving encoding (the inverse of order_bits)
+    const unsigned long long rl = (bl >> 63) ? (bl & 0x7FFFFFFFFFFFFFFFull) : ~bl;
+    const unsigned long long rh = (bh >> 63) ? (bh & 0x7FFFFFFFFFFFFFFFull) : ~bh;
+    std::memcpy(&lo, &rl, sizeof(lo));
+    std::memcpy(&hi, &rh, sizeof(hi));
+    if (!std::isfinite(lo) || !std::isfinite(hi) || lo > hi || !std::isfinite(hi - lo))
+      return fail(NBB_ERR_INVALID_ARGUMENT, "Position frame bounds must be finite and ordered");
+  }
+  NBB_CUDA(cudaMemcpyAsync(out, fb.frame, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st),
+           "Could not copy quantized samples to the frame writer");
+  NBB_CUDA(cudaStreamSynchronize(st), "Could not copy quantized samples to the frame writer");
+  if (written) *written = bytes;
   return ok();
 }
 

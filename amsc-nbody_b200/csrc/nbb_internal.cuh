@@ -324,6 +324,23 @@ struct FrozenBatch {
   int *pparent = nullptr;      // cap_nodes
   int2 *prange = nullptr;      // cap_nodes
 };
+// Frame capture (capture.cu): device scalars and header fields.
+constexpr unsigned long long kFrameHeaderBytes = 128;  // version-3 header
+struct FrameScalars {
+  unsigned long long lo[3], hi[3];  // order-preserving encoded extrema
+  int nonfinite;                    // a sampled position is not finite
+  int bad_type;                     // a sampled type is outside 0..4
+};
+struct FrameHeaderFields {
+  unsigned long long sequence = 0, step = 0, source_count = 0, sample_count = 0;
+  double time = 0.0;
+};
+// Sample s of n particles ((i * n) / s), bounds, quantized payload and
+// header into `frame` (kFrameHeaderBytes + 7 s bytes); flags in f.
+cudaError_t launch_frame_capture(const double *x, const double *y, const double *z, const uint8_t *type, size_t n,
+                                 size_t s, FrameScalars *f, const FrameHeaderFields &h, unsigned char *frame,
+                                 cudaStream_t st);
+
 // VJP of the plain FP64 force on the current tree (built from the positions
 // in the workspace): accumulates into ab.gx / gy / gz / gm.
 cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,

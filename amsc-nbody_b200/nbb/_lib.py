@@ -91,6 +91,8 @@ SIGNATURES = {
     "nbb_radix_tree": (_I, [_P, _I] + [_P] * 6),
     "nbb_measure_fma_tflops": (_I, [_I, _P]),
     "nbb_selftest_bounded_wait": (_I, []),
+    "nbb_frame_bytes": (_Z, [_P, _Z]),
+    "nbb_sim_capture_frame": (_I, [_P, _Z, C.c_uint64, _P, _Z, _P, _I]),
     "nbb_sim_rollout": (_I, [_P, C.c_uint64, C.c_uint64]),
     "nbb_sim_backward": (_I, [_P] * 14 + [_I]),
     "nbb_frozen_rollout": (_I, [_P, _Z] + [_P] * 7 + [_Z] + [_P] * 7 + [C.c_uint64] + [_P] * 6 + [_I]),

@@ -57,14 +57,15 @@ class Simulation:
     """Owns the particle state on the GPU and advances it with leapfrog KDK
     (src/simulation.cpp:286-343).  ``particles`` is copied in."""
 
-    def __init__(self, particles: ParticleData, config: SimulationConfig):
+    def __init__(self, particles: ParticleData, config: SimulationConfig, types=None):
         lib = _lib.load()
         self._lib = lib
         self._handle = C.c_void_p()
         self._n = len(particles)
         arrs = [_f64(a) for a in particles.arrays()]
+        t = None if types is None else np.ascontiguousarray(types, dtype=np.uint8)
         cfg = config.to_c()
-        check(lib.nbb_sim_create(C.byref(cfg), self._n, *[ptr(a) for a in arrs], None, 0,
+        check(lib.nbb_sim_create(C.byref(cfg), self._n, *[ptr(a) for a in arrs], ptr(t), 0,
                                  C.byref(self._handle)))
         self.config = config
 
@@ -147,6 +148,16 @@ class Simulation:
         st = _lib.Stats()
         check(self._lib.nbb_sim_profile(self._handle, ms, C.byref(st)))
         return dict(zip(self.PROFILE_STAGES, list(ms))), st
+
+    def capture_frame(self, max_particles: int = 100000, sequence: int = 0) -> bytes:
+        """Quantized frame of the current positions (nbb_sim_capture_frame),
+        in the reference's version-3 .nbsnap layout; see nbb.frames."""
+        size = self._lib.nbb_frame_bytes(self._handle, int(max_particles))
+        buf = np.empty(size, np.uint8)
+        written = C.c_size_t(0)
+        check(self._lib.nbb_sim_capture_frame(self._handle, int(max_particles), int(sequence), ptr(buf), size,
+                                              C.byref(written), 0))
+        return buf[: written.value].tobytes()
 
     def rollout(self, steps: int, checkpoint_every: int = 32) -> None:
         """Advance ``steps`` steps keeping (x, v, a) every

@@ -271,6 +271,24 @@ const char *nbb_noalloc_last_error_message(void);
 int nbb_selftest_bounded_wait(void);
 
 /* ---------------------------------------------------------------------------
+ * Frame capture (src/streaming/device_capture.hpp:12-35 DeviceFrameWriter and
+ * src/streaming/frame.cpp:341-470 writeQuantizedPositions): a quantized
+ * snapshot of the current positions as one byte buffer in the reference's
+ * version-3 frame layout -- 128-byte little-endian header ("NBSNAP01",
+ * version, header size, sequence, step, time, source and sample counts,
+ * scalar bytes 2, components 3, payload bytes, bounds min/max, type bytes),
+ * then 3 x uint16 per sample, then one uint8 particle type per sample (0 when
+ * the simulation has no types).  max_particles 0 (or >= count) samples every
+ * particle, otherwise sample i is particle (i * count) / max_particles.
+ * nbb_frame_bytes gives the buffer size needed.  Errors as the reference:
+ * NBB_ERR_DOMAIN for a non-finite sampled position, NBB_ERR_INVALID_ARGUMENT
+ * for an invalid type or a buffer that is too small.  The frame is built on
+ * the device; `out` is host memory unless on_device. */
+size_t nbb_frame_bytes(const nbb_sim *sim, size_t max_particles);
+int nbb_sim_capture_frame(nbb_sim *sim, size_t max_particles, uint64_t sequence, void *out, size_t capacity,
+                          size_t *written, int on_device);
+
+/* ---------------------------------------------------------------------------
  * Differentiable rollout.  No counterpart in the reference (which has no
  * derivative of its step); the force differentiated is the plain FP64
  * Barnes-Hut force of src/barnes_hut.cu:184-342 with the tree topology and

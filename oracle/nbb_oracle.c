@@ -896,3 +896,75 @@ int orc_simulate(size_t n, const double *m, double *x, double *y, double *z,
   free(b.block);
   return st;
 }
+
+/* ------------------------------------------------------- frame capture */
+
+static unsigned char *put_le(unsigned char *p, uint64_t v, int bytes) {
+  for (int b = 0; b < bytes; ++b) p[b] = (unsigned char)((v >> (8 * b)) & 0xffu);
+  return p + bytes;
+}
+
+static unsigned char *put_f64(unsigned char *p, double v) {
+  uint64_t bits;
+  memcpy(&bits, &v, sizeof(bits));
+  return put_le(p, bits, 8);
+}
+
+/* device_capture.cu:118-126 as nvcc compiles it (the product plus one half
+ * is a fused multiply-add). */
+static uint16_t frame_quantize(double p, double lo, double hi) {
+  if (hi == lo) return 0;
+  double u = (p - lo) / (hi - lo);
+  u = fmin(1.0, fmax(0.0, u));
+  return (uint16_t)fma(u, 65535.0, 0.5);
+}
+
+long long orc_frame_capture(size_t n, const double *x, const double *y, const double *z,
+                            const uint8_t *type, size_t max_particles, uint64_t sequence,
+                            uint64_t step, double time, unsigned char *out, size_t cap) {
+  if (n == 0 || !x || !y || !z || !out || !isfinite(time) || time < 0.0) return -1;
+  const size_t s = (max_particles == 0 || max_particles > n) ? n : max_particles;
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  const double *c[3] = {x, y, z};
+  for (size_t i = 0; i < s; ++i) {
+    const size_t src = (size_t)(((unsigned long long)i * n) / s);
+    const double v[3] = {x[src], y[src], z[src]};
+    if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) return -2;
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = fmin(lo[a], v[a]);
+      hi[a] = fmax(hi[a], v[a]);
+    }
+  }
+  for (int a = 0; a < 3; ++a)
+    if (!isfinite(lo[a]) || !isfinite(hi[a]) || lo[a] > hi[a] || !isfinite(hi[a] - lo[a])) return -4;
+  if (type)
+    for (size_t i = 0; i < s; ++i)
+      if (type[(size_t)(((unsigned long long)i * n) / s)] > 4) return -3;
+  const size_t header = type ? 128 : 120;
+  const size_t type_bytes = type ? s : 0;
+  const size_t total = header + 6 * s + type_bytes;
+  if (cap < total) return -5;
+  unsigned char *p = out;
+  memcpy(p, "NBSNAP01", 8);
+  p += 8;
+  p = put_le(p, type ? 3u : 2u, 4);
+  p = put_le(p, header, 4);
+  p = put_le(p, sequence, 8);
+  p = put_le(p, step, 8);
+  p = put_f64(p, time);
+  p = put_le(p, n, 8);
+  p = put_le(p, s, 8);
+  p = put_le(p, 2, 4);
+  p = put_le(p, 3, 4);
+  p = put_le(p, 6 * s + type_bytes, 8);
+  for (int a = 0; a < 3; ++a) p = put_f64(p, lo[a]);
+  for (int a = 0; a < 3; ++a) p = put_f64(p, hi[a]);
+  if (type) p = put_le(p, type_bytes, 8);
+  for (size_t i = 0; i < s; ++i) {
+    const size_t src = (size_t)(((unsigned long long)i * n) / s);
+    for (int a = 0; a < 3; ++a) p = put_le(p, frame_quantize(c[a][src], lo[a], hi[a]), 2);
+  }
+  if (type)
+    for (size_t i = 0; i < s; ++i) *p++ = type[(size_t)(((unsigned long long)i * n) / s)];
+  return (long long)total;
+}

@@ -152,6 +152,19 @@ int orc_simulate(size_t n, const double *m, double *x, double *y, double *z,
                  double *az, double dt, double theta, double soft, double g,
                  int steps, int n_threads);
 
+/* Quantized position frame of the current state (src/streaming/
+ * device_capture.cu:27-330 for sampling, bounds and quantization;
+ * src/streaming/frame.cpp:68-95, 341-470 for the byte layout).  Samples
+ * s = max_particles (0 or more than n: all) particles at source indices
+ * (i * n) / s; writes the frame -- a 128-byte (types given) or 120-byte
+ * header, 3 x uint16 per sample, then one uint8 type per sample -- into out
+ * (capacity cap bytes) and returns its size, or a negative status: -1
+ * argument, -2 non-finite sampled position, -3 invalid particle type,
+ * -4 bounds not finite, -5 capacity too small. */
+long long orc_frame_capture(size_t n, const double *x, const double *y, const double *z,
+                            const uint8_t *type, size_t max_particles, uint64_t sequence,
+                            uint64_t step, double time, unsigned char *out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,20 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(_P)
 
 
+def frame_capture(x, y, z, types=None, max_particles=0, sequence=0, step=0, time=0.0):
+    """orc_frame_capture: the frame's bytes, or raises ValueError(status)."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    n = x.size
+    s = n if (max_particles == 0 or max_particles > n) else max_particles
+    t = None if types is None else np.ascontiguousarray(types, dtype=np.uint8)
+    out = np.zeros(128 + 7 * s, np.uint8)
+    r = lib().orc_frame_capture(n, _ptr(x), _ptr(y), _ptr(z), _ptr(t), int(max_particles), int(sequence),
+                                int(step), float(time), _ptr(out), out.size)
+    if r < 0:
+        raise ValueError(r)
+    return out[:r].tobytes()
+
+
 def build_oracle() -> str:
     if not os.path.exists(ORACLE_SO):
         subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
@@ -57,6 +71,8 @@ def lib():
         L.orc_kick.restype = None
         L.orc_pipeline.argtypes = [_Z, _P, _P, _P, _P, _D, _D, _D, _I, _P]
         L.orc_simulate.argtypes = [_Z] + [_P] * 10 + [_D, _D, _D, _D, _I, _I]
+        L.orc_frame_capture.argtypes = [_Z, _P, _P, _P, _P, _Z, C.c_uint64, C.c_uint64, _D, _P, _Z]
+        L.orc_frame_capture.restype = C.c_longlong
     return _lib
 
 
@@ -324,7 +340,24 @@ def ref_lib():
         _ref.ref_simulate.argtypes = [_Z] + [_P] * 10 + [_D, _D, _D, _D, _I, _P]
         _ref.ref_radix_tree.argtypes = [_I, _P, _P, _P, _P, _P, _P, _P]
         _ref.ref_last_error.restype = C.c_char_p
+        _ref.ref_capture_frame.argtypes = [_Z, _P, _P, _P, _P, _Z, C.c_uint64, C.c_uint64, _D, C.c_char_p,
+                                           C.c_char_p, _Z]
+        _ref.ref_capture_last_error.restype = C.c_char_p
     return _ref
+
+
+def ref_capture_frame(x, y, z, types, max_particles, sequence, step, time, directory):
+    """The reference's DeviceFrameWriter + FrameSpool: returns the frame file's
+    bytes (written under `directory`), or raises with the reference's message."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    t = np.ascontiguousarray(types, dtype=np.uint8)
+    path = C.create_string_buffer(4096)
+    st = ref_lib().ref_capture_frame(x.size, _ptr(x), _ptr(y), _ptr(z), _ptr(t), int(max_particles),
+                                     int(sequence), int(step), float(time), directory.encode(), path, 4096)
+    if st:
+        raise RuntimeError(ref_lib().ref_capture_last_error().decode())
+    with open(path.value.decode(), "rb") as f:
+        return f.read()
 
 
 class _RefOut(C.Structure):

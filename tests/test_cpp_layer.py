@@ -76,3 +76,34 @@ def test_cpp_simulation_layer(tmp_path, nbb_mod):
     out = subprocess.run([exe], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     assert out.stdout.strip() == "ok"
+
+
+def test_cli_frame_option_handling(tmp_path):
+    # apps/simulation/main.cpp:165-205: frame options; the stream server is not built
+    r = _run_cli("--input", "x.bin", "--time-step", "0.25", "--steps", "1", "--sample-rate", "0")
+    assert r.returncode == 2 and "--sample-rate must be positive" in r.stderr
+    r = _run_cli("--input", "x.bin", "--time-step", "0.25", "--steps", "1", "--stream-max-particles", "-3")
+    assert r.returncode == 2 and "--stream-max-particles" in r.stderr
+    r = _run_cli("--input", "x.bin", "--time-step", "0.25", "--steps", "1", "--cluster")
+    assert r.returncode == 2 and "not part of this build" in r.stderr
+    r = _run_cli("--help")
+    assert "--stream-dir DIR" in r.stdout and "--sample-rate HZ" in r.stdout
+
+
+@pytest.mark.gpu
+def test_cli_writes_frames(tmp_path, nbb_mod):
+    from nbb import frames
+
+    path = tmp_path / "one.bin"
+    write_one_particle(path)
+    spool = tmp_path / "spool"
+    r = _run_cli("--input", str(path), "--time-step", "0.25", "--steps", "3", "--stream-dir", str(spool),
+                 "--sample-rate", "1000000")
+    assert r.returncode == 0, r.stderr
+    assert "frames written: 4" in r.stdout and "particles per frame: 1 of 1" in r.stdout
+    names = sorted(os.listdir(spool))
+    snaps = [n for n in names if n.endswith(".nbsnap")]
+    assert len(snaps) == 4 and any(n.endswith(".complete") for n in names)
+    with open(spool / snaps[-1], "rb") as f:
+        h = frames.read_header(f.read())
+    assert (h["version"], h["sequence"], h["simulation_step"], h["simulation_time"]) == (3, 3, 3, 0.75)
