@@ -363,6 +363,13 @@ struct FrameBuffers {
   FrameScalars *scalars = nullptr;
 };
 
+// Device buffers of the conserved-quantity monitor, taken at its first use.
+struct DiagBuffers {
+  static constexpr int kBlocks = 592;  // fixed: the sums' order never changes
+  Allocation al;
+  double *partials = nullptr, *out = nullptr, *phi = nullptr;
+};
+
 struct nbb_sim {
   nbb_config cfg{};
   Workspace ws{};
@@ -379,6 +386,7 @@ struct nbb_sim {
   double min_softening = 0.0;  // ensembles: smallest per-system softening
   std::unique_ptr<RolloutRecord> rollout;
   std::unique_ptr<FrameBuffers> frames;
+  std::unique_ptr<DiagBuffers> diag;
 };
 
 extern "C" {
@@ -1486,6 +1494,71 @@ int nbb_sim_capture_frame(nbb_sim *sim, size_t max_particles, uint64_t sequence,
            "Could not copy quantized samples to the frame writer");
   NBB_CUDA(cudaStreamSynchronize(st), "Could not copy quantized samples to the frame writer");
   if (written) *written = bytes;
+  return ok();
+}
+
+}  // extern "C"
+
+// -------------------------------------------------- conserved quantities --
+
+extern "C" {
+
+int nbb_sim_diagnostics(nbb_sim *sim, int potential, nbb_diagnostics *d) {
+  if (!sim || !d) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  if (potential < NBB_POTENTIAL_NONE || potential > NBB_POTENTIAL_DIRECT)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "unknown potential mode");
+  if (sim->state == nbb_sim::State::failed) return fail(NBB_ERR_LOGIC, "Simulation is in a failed state");
+  Workspace &ws = sim->ws;
+  if (potential == NBB_POTENTIAL_DIRECT && ws.n_systems > 1)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "direct potential of an ensemble is not defined; use the tree potential");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  const size_t n = (size_t)ws.n;
+  if (!sim->diag) {
+    auto db = std::make_unique<DiagBuffers>();
+    NBB_CUDA(db->al.get(db->partials, (size_t)DiagBuffers::kBlocks * 12), "diagnostics allocation");
+    NBB_CUDA(db->al.get(db->out, 12), "diagnostics allocation");
+    NBB_CUDA(db->al.get(db->phi, n), "diagnostics allocation");
+    sim->diag = std::move(db);
+  }
+  DiagBuffers &db = *sim->diag;
+  cudaStream_t s = sim->stream;
+  const double *phi = nullptr;
+  if (potential == NBB_POTENTIAL_TREE) {
+    // the tree of the current positions (the handle's last tree may belong
+    // to other positions, e.g. after a backward pass)
+    TraversalParams tp = traversal_params(sim, 0);
+    tp.precision = 0;
+    tp.group_mode = ws.n_systems > 1 ? 1 : 0;
+    cudaError_t e = launch_step_reset(ws, s);
+    if (e == cudaSuccess) e = launch_kd_bbox(ws, 0.0, 0, s);
+    if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
+    if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
+    if (e == cudaSuccess) e = launch_potential_tree(ws, tp, db.phi, s);
+    NBB_CUDA(e, "potential evaluation");
+    phi = db.phi;
+  } else if (potential == NBB_POTENTIAL_DIRECT) {
+    NBB_CUDA(launch_potential_direct(ws.m, ws.x, ws.y, ws.z, (int)n, sim->cfg.gravitational_constant,
+                                     sim->cfg.softening, db.phi, s),
+             "potential evaluation");
+    phi = db.phi;
+  }
+  NBB_CUDA(launch_moments(ws.m, ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz, phi, n, db.partials, DiagBuffers::kBlocks,
+                          db.out, s),
+           "moments");
+  double h[12];
+  NBB_CUDA(cudaMemcpyAsync(h, db.out, sizeof(h), cudaMemcpyDeviceToHost, s), "copy diagnostics");
+  const int st = check_device(ws, s);
+  if (st) return st;
+  d->mass = h[0];
+  for (int a = 0; a < 3; ++a) {
+    d->center_of_mass[a] = h[0] != 0.0 ? h[1 + a] / h[0] : 0.0;
+    d->momentum[a] = h[4 + a];
+    d->angular_momentum[a] = h[7 + a];
+  }
+  d->kinetic_energy = h[10];
+  d->potential_energy = potential ? h[11] : 0.0;
+  d->total_energy = d->kinetic_energy + d->potential_energy;
+  d->potential = potential;
   return ok();
 }
 

@@ -341,6 +341,18 @@ cudaError_t launch_frame_capture(const double *x, const double *y, const double 
                                  size_t s, FrameScalars *f, const FrameHeaderFields &h, unsigned char *frame,
                                  cudaStream_t st);
 
+// Conserved quantities (diagnostics.cu): 12 sums -- m, m x (3), m v (3),
+// m x cross v (3), kinetic energy, 1/2 m phi -- over n particles (phi may be
+// null), block partials then one fixed-order final sum into out[12].
+cudaError_t launch_moments(const double *m, const double *x, const double *y, const double *z, const double *vx,
+                           const double *vy, const double *vz, const double *phi, size_t n, double *partials,
+                           int blocks, double *out, cudaStream_t s);
+// Potential of every particle (original order) from the current tree, with
+// the plain walk's acceptance test; and by direct summation.
+cudaError_t launch_potential_tree(Workspace &ws, const TraversalParams &p, double *phi, cudaStream_t s);
+cudaError_t launch_potential_direct(const double *m, const double *x, const double *y, const double *z, int n,
+                                    double g, double soft, double *phi, cudaStream_t s);
+
 // VJP of the plain FP64 force on the current tree (built from the positions
 // in the workspace): accumulates into ab.gx / gy / gz / gm.
 cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,

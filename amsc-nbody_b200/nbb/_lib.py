@@ -56,6 +56,14 @@ class TreeExport(C.Structure):
                           "comz")] + [("n_groups", C.c_int), ("n_octree", C.c_int)]
 
 
+class Diagnostics(C.Structure):
+    _fields_ = [("mass", _D), ("center_of_mass", _D * 3), ("momentum", _D * 3), ("angular_momentum", _D * 3),
+                ("kinetic_energy", _D), ("potential_energy", _D), ("total_energy", _D), ("potential", _I)]
+
+
+POTENTIAL_NONE, POTENTIAL_TREE, POTENTIAL_DIRECT = 0, 1, 2
+
+
 class OctreeView(C.Structure):
     _fields_ = [("n_nodes", C.c_int), ("n_particles", C.c_int)] + [(f, _P) for f in (
         "children", "parent", "first", "count", "mass", "comx", "comy", "comz", "cx", "cy", "cz",
@@ -91,6 +99,7 @@ SIGNATURES = {
     "nbb_radix_tree": (_I, [_P, _I] + [_P] * 6),
     "nbb_measure_fma_tflops": (_I, [_I, _P]),
     "nbb_selftest_bounded_wait": (_I, []),
+    "nbb_sim_diagnostics": (_I, [_P, _I, _P]),
     "nbb_frame_bytes": (_Z, [_P, _Z]),
     "nbb_sim_capture_frame": (_I, [_P, _Z, C.c_uint64, _P, _Z, _P, _I]),
     "nbb_sim_rollout": (_I, [_P, C.c_uint64, C.c_uint64]),

@@ -149,6 +149,17 @@ class Simulation:
         check(self._lib.nbb_sim_profile(self._handle, ms, C.byref(st)))
         return dict(zip(self.PROFILE_STAGES, list(ms))), st
 
+    def diagnostics(self, potential: int = _lib.POTENTIAL_TREE) -> dict:
+        """Conserved quantities of the current state (nbb_sim_diagnostics):
+        mass, centre of mass, momentum, angular momentum, kinetic, potential
+        and total energy."""
+        d = _lib.Diagnostics()
+        check(self._lib.nbb_sim_diagnostics(self._handle, int(potential), C.byref(d)))
+        return {"mass": d.mass, "center_of_mass": np.array(d.center_of_mass[:]),
+                "momentum": np.array(d.momentum[:]), "angular_momentum": np.array(d.angular_momentum[:]),
+                "kinetic_energy": d.kinetic_energy, "potential_energy": d.potential_energy,
+                "total_energy": d.total_energy}
+
     def capture_frame(self, max_particles: int = 100000, sequence: int = 0) -> bytes:
         """Quantized frame of the current positions (nbb_sim_capture_frame),
         in the reference's version-3 .nbsnap layout; see nbb.frames."""
@@ -426,3 +437,35 @@ def direct_rollout_adjoint(particles: ParticleData, config: SimulationConfig, st
                                          ptr(gm), *[ptr(gx0[k]) for k in range(3)],
                                          *[ptr(gv0[k]) for k in range(3)], 0))
     return final, gm, gx0, gv0
+
+
+class ConservationMonitor:
+    """Relative drift of the conserved quantities of a simulation over time:
+    ``record()`` stores the current diagnostics; ``drift()`` gives, for the
+    last record, |E - E0| / |E0| for the total energy and |P - P0| / scale,
+    |L - L0| / scale for momentum and angular momentum (scale: their initial
+    norms, or sum m |v| and sum m |x| |v| when those vanish)."""
+
+    def __init__(self, simulation: Simulation, potential: int = _lib.POTENTIAL_TREE):
+        self.sim = simulation
+        self.potential = potential
+        self.records = []
+
+    def record(self) -> dict:
+        d = self.sim.diagnostics(self.potential)
+        d["step"] = self.sim.step_number()
+        d["time"] = self.sim.time()
+        self.records.append(d)
+        return d
+
+    def drift(self) -> dict:
+        if not self.records:
+            raise ValueError("no diagnostics recorded")
+        d0, d = self.records[0], self.records[-1]
+        e0 = abs(d0["total_energy"]) or 1.0
+        p_scale = np.linalg.norm(d0["momentum"]) or 1.0
+        l_scale = np.linalg.norm(d0["angular_momentum"]) or 1.0
+        return {"energy": abs(d["total_energy"] - d0["total_energy"]) / e0,
+                "momentum": float(np.linalg.norm(d["momentum"] - d0["momentum"]) / p_scale),
+                "angular_momentum": float(np.linalg.norm(d["angular_momentum"] - d0["angular_momentum"]) / l_scale),
+                "steps": d["step"] - d0["step"]}

@@ -289,6 +289,28 @@ int nbb_sim_capture_frame(nbb_sim *sim, size_t max_particles, uint64_t sequence,
                           size_t *written, int on_device);
 
 /* ---------------------------------------------------------------------------
+ * Conserved-quantity monitor (the reference lists total energy, linear and
+ * angular momentum monitoring as planned work, README.md:766-774): sums over
+ * the current state, each in a fixed order (repeatable bit for bit).  The
+ * potential energy 1/2 sum m_i phi_i is optional: NBB_POTENTIAL_TREE
+ * evaluates phi with the Barnes-Hut acceptance test of the plain form on a
+ * tree rebuilt at the current positions (the cost of one FP64 force
+ * evaluation), NBB_POTENTIAL_DIRECT by all pairs (O(N^2); not for
+ * ensembles).  For an ensemble the sums run over all systems. */
+enum { NBB_POTENTIAL_NONE = 0, NBB_POTENTIAL_TREE = 1, NBB_POTENTIAL_DIRECT = 2 };
+typedef struct nbb_diagnostics {
+  double mass;
+  double center_of_mass[3];
+  double momentum[3];          /* sum m v */
+  double angular_momentum[3];  /* sum m x cross v, about the origin */
+  double kinetic_energy;       /* sum 1/2 m |v|^2 */
+  double potential_energy;     /* 0 unless requested */
+  double total_energy;
+  int potential;               /* the mode used */
+} nbb_diagnostics;
+int nbb_sim_diagnostics(nbb_sim *sim, int potential, nbb_diagnostics *out);
+
+/* ---------------------------------------------------------------------------
  * Differentiable rollout.  No counterpart in the reference (which has no
  * derivative of its step); the force differentiated is the plain FP64
  * Barnes-Hut force of src/barnes_hut.cu:184-342 with the tree topology and
