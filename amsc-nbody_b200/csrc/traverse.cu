@@ -140,8 +140,11 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
 #ifndef NBB_MIXED_MINBLOCKS
 #define NBB_MIXED_MINBLOCKS 12
 #endif
-// resident blocks per SM for the four-targets-per-lane instance (more
-// registers per thread for the targets' sums)
+// resident blocks per SM for the two- and four-targets-per-lane instances
+// (more registers per thread for the targets' sums)
+#ifndef NBB_MIXED_MINBLOCKS2
+#define NBB_MIXED_MINBLOCKS2 10
+#endif
 #ifndef NBB_MIXED_MINBLOCKS4
 #define NBB_MIXED_MINBLOCKS4 8
 #endif
@@ -149,10 +152,28 @@ constexpr int kMixedWarps = NBB_MIXED_WARPS;
 constexpr int kStackCap = 512;
 constexpr int kListCap = 96;
 
+// The interaction list keeps entries in pairs so that packed two-wide FP32
+// instructions (sm_100's FADD2 / FMUL2 / FFMA2) evaluate two entries at once
+// from one 16-byte load per half: pair p holds entries 2p and 2p + 1 as
+// a = {x0, x1, y0, y1} and b = {z0, z1, m0, m1}.
+struct PairList {
+  float4 *a, *b;
+  __device__ __forceinline__ void put(int j, float x, float y, float z, float m) const {
+    float *pa = reinterpret_cast<float *>(a + (j >> 1));
+    float *pb = reinterpret_cast<float *>(b + (j >> 1));
+    const int h = j & 1;
+    pa[h] = x;
+    pa[2 + h] = y;
+    pb[h] = z;
+    pb[2 + h] = m;
+  }
+};
+
 template <bool kTrackSource>
 struct MixedShared {
   int stack[kMixedWarps][kStackCap];
-  float4 list[kMixedWarps][kListCap];
+  float4 la[kMixedWarps][kListCap / 2];
+  float4 lb[kMixedWarps][kListCap / 2];
   int src[kMixedWarps][kTrackSource ? kListCap : 1];
 };
 
@@ -166,10 +187,11 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return r;
 }
 
-// Evaluate `count` list entries for this lane's kTPL targets: FP32 offsets,
-// approximate rsqrt plus one Newton step, plain FP32 partial sums over the
-// batch, then one Kahan-compensated addition of each batch partial into its
-// running sum.
+// Evaluate `count` list entries (rounded up to a whole pair; an odd count
+// has a zero-mass pad after it) for this lane's kTPL targets: FP32 offsets,
+// approximate rsqrt plus one Newton step, two-wide FP32 partial sums over
+// the batch, then one Kahan-compensated addition of each batch partial into
+// its running sum.
 //
 // With positive softening a target's own entry (a leaf particle equal to the
 // target) has offset exactly (0, 0, 0) -- both offsets are rounded from the
@@ -177,49 +199,55 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 // needed.  With zero softening the source index excludes self and detects
 // the reference's singular interaction (returns true).
 template <bool kTrackSource, int kTPL>
-__device__ __forceinline__ bool eval_batch(const float4 *list, const int *src, int count, const int *self,
-                                           const float *tx, const float *ty, const float *tz, float eps2,
+__device__ __forceinline__ bool eval_batch(const PairList &list, const int *src, int count, const int *self,
+                                           const float2 *ntx, const float2 *nty, const float2 *ntz, float2 eps2,
                                            float3 *sum, float3 *comp) {
-  float px[kTPL], py[kTPL], pz[kTPL];
+  float2 px[kTPL], py[kTPL], pz[kTPL];
 #pragma unroll
-  for (int q = 0; q < kTPL; ++q) px[q] = py[q] = pz[q] = 0.f;
+  for (int q = 0; q < kTPL; ++q) px[q] = py[q] = pz[q] = make_float2(0.f, 0.f);
+  const float2 neg_half = make_float2(-0.5f, -0.5f), three_halves = make_float2(1.5f, 1.5f);
   bool singular = false;
-#pragma unroll 8
-  for (int j = 0; j < count; ++j) {
-    const float4 e = list[j];
+  const int pairs = (count + 1) >> 1;
+#pragma unroll 4
+  for (int pr = 0; pr < pairs; ++pr) {
+    const float4 ea = list.a[pr], eb = list.b[pr];
+    const float2 ex = make_float2(ea.x, ea.y), ey = make_float2(ea.z, ea.w);
+    const float2 ez = make_float2(eb.x, eb.y), em = make_float2(eb.z, eb.w);
 #pragma unroll
     for (int q = 0; q < kTPL; ++q) {
-      const float dx = e.x - tx[q], dy = e.y - ty[q], dz = e.z - tz[q];
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-      float r = rsqrt_approx(r2);
-      r = r * fmaf(-0.5f * r2, r * r, 1.5f);
-      float f = e.w * (r * r * r);
+      const float2 dx = __fadd2_rn(ex, ntx[q]), dy = __fadd2_rn(ey, nty[q]), dz = __fadd2_rn(ez, ntz[q]);
+      const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+      float2 r = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+      r = __fmul2_rn(r, __ffma2_rn(__fmul2_rn(neg_half, r2), __fmul2_rn(r, r), three_halves));
+      float2 f = __fmul2_rn(em, __fmul2_rn(__fmul2_rn(r, r), r));
       if (kTrackSource) {
-        const bool other = src[j] != self[q];
-        singular |= other && !(r2 > 0.f) && e.w != 0.f;
-        f = (other && r2 > 0.f) ? f : 0.f;
+        const bool o0 = src[2 * pr] != self[q], o1 = src[2 * pr + 1] != self[q];
+        singular |= (o0 && !(r2.x > 0.f) && em.x != 0.f) || (o1 && !(r2.y > 0.f) && em.y != 0.f);
+        f.x = (o0 && r2.x > 0.f) ? f.x : 0.f;
+        f.y = (o1 && r2.y > 0.f) ? f.y : 0.f;
       }
-      px[q] = fmaf(f, dx, px[q]);
-      py[q] = fmaf(f, dy, py[q]);
-      pz[q] = fmaf(f, dz, pz[q]);
+      px[q] = __ffma2_rn(f, dx, px[q]);
+      py[q] = __ffma2_rn(f, dy, py[q]);
+      pz[q] = __ffma2_rn(f, dz, pz[q]);
     }
   }
 #pragma unroll
   for (int q = 0; q < kTPL; ++q) {
     float y, t;
-    y = px[q] - comp[q].x; t = sum[q].x + y; comp[q].x = (t - sum[q].x) - y; sum[q].x = t;
-    y = py[q] - comp[q].y; t = sum[q].y + y; comp[q].y = (t - sum[q].y) - y; sum[q].y = t;
-    y = pz[q] - comp[q].z; t = sum[q].z + y; comp[q].z = (t - sum[q].z) - y; sum[q].z = t;
+    y = (px[q].x + px[q].y) - comp[q].x; t = sum[q].x + y; comp[q].x = (t - sum[q].x) - y; sum[q].x = t;
+    y = (py[q].x + py[q].y) - comp[q].y; t = sum[q].y + y; comp[q].y = (t - sum[q].y) - y; sum[q].y = t;
+    y = (pz[q].x + pz[q].y) - comp[q].z; t = sum[q].z + y; comp[q].z = (t - sum[q].z) - y; sum[q].z = t;
   }
   return singular;
 }
 
-// Per-lane target state of the mixed walk.
+// Per-lane target state of the mixed walk: negated target offsets from the
+// group centre, each duplicated into both halves of a pair.
 template <int kTPL>
 struct LaneTargets {
   int s[kTPL];
   bool valid[kTPL];
-  float tx[kTPL], ty[kTPL], tz[kTPL];
+  float2 ntx[kTPL], nty[kTPL], ntz[kTPL];
   float3 sum[kTPL], comp[kTPL];
   long long inter = 0;
   bool singular = false;
@@ -230,30 +258,28 @@ struct LaneTargets {
 // empty ones cost nothing (the branch is taken once per batch, outside the
 // entry loop).
 template <bool kTrackSource, int kTPL>
-__device__ __forceinline__ bool eval_slots(const float4 *list, const int *src, int count, int nq,
-                                           LaneTargets<kTPL> &t, float eps2) {
+__device__ __forceinline__ bool eval_slots(const PairList &list, const int *src, int count, int nq,
+                                           LaneTargets<kTPL> &t, float2 eps2) {
   if (kTPL >= 4 && nq >= 4)
-    return eval_batch<kTrackSource, (kTPL >= 4 ? 4 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 4 ? 4 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
   if (kTPL >= 3 && nq == 3)
-    return eval_batch<kTrackSource, (kTPL >= 3 ? 3 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 3 ? 3 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
   if (kTPL >= 2 && nq == 2)
-    return eval_batch<kTrackSource, (kTPL >= 2 ? 2 : 1)>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 2 ? 2 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
-  return eval_batch<kTrackSource, 1>(list, src, count, t.s, t.tx, t.ty, t.tz, eps2, t.sum, t.comp);
+  return eval_batch<kTrackSource, 1>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum, t.comp);
 }
 
-// Evaluate full batches of 32 from the front of the list, shifting the
-// remainder down, until fewer than 32 entries are left.
 template <bool kTrackSource, int kTPL>
-__device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, LaneTargets<kTPL> &lt_,
-                                           float eps2, int nq) {
+__device__ __forceinline__ void flush_full(const PairList &list, int *src, int &ls, LaneTargets<kTPL> &lt_,
+                                           float2 eps2, int nq) {
   const int lane = threadIdx.x & 31;
   int done = 0;
   while (ls - done >= 32) {
-    const bool sg = eval_slots<kTrackSource, kTPL>(list + done, src + (kTrackSource ? done : 0), 32, nq, lt_,
-                                                   eps2);
+    const PairList part{list.a + done / 2, list.b + done / 2};
+    const bool sg = eval_slots<kTrackSource, kTPL>(part, src + (kTrackSource ? done : 0), 32, nq, lt_, eps2);
 #pragma unroll
     for (int q = 0; q < kTPL; ++q)
       if (lt_.valid[q]) {
@@ -265,10 +291,11 @@ __device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, Lane
   if (done) {
     __syncwarp();
     const int rest = ls - done;
-    if (lane < rest) {
-      list[lane] = list[done + lane];
-      if (kTrackSource) src[lane] = src[done + lane];
+    if (lane < (rest + 1) / 2) {
+      list.a[lane] = list.a[done / 2 + lane];
+      list.b[lane] = list.b[done / 2 + lane];
     }
+    if (kTrackSource && lane < rest) src[lane] = src[done + lane];
     ls = rest;
     __syncwarp();
   }
@@ -287,7 +314,8 @@ __device__ __forceinline__ void flush_full(float4 *list, int *src, int &ls, Lane
 // group centre (formed in FP64, then rounded) and are evaluated by all lanes
 // in batches of 32.
 template <bool kTrackSource, int kTPL>
-__global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : NBB_MIXED_MINBLOCKS)
+__global__ void __launch_bounds__(kMixedWarps * 32,
+                                   kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : (kTPL == 2 ? NBB_MIXED_MINBLOCKS2 : NBB_MIXED_MINBLOCKS))
     traverse_mixed_kernel(Workspace ws, TraversalParams p) {
   __shared__ MixedShared<kTrackSource> sh;
   DevScalars *sc = ws.sc;
@@ -295,7 +323,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
   const int lane = threadIdx.x & 31;
   const int wid = threadIdx.x >> 5;
   int *stack = sh.stack[wid];
-  float4 *list = sh.list[wid];
+  const PairList list{sh.la[wid], sh.lb[wid]};
   int *src = sh.src[wid];
   const int n = ws.n;
   const int m = sc->n_nodes;
@@ -342,17 +370,27 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
     }
     const double gcx = 0.5 * (lo[0] + hi[0]), gcy = 0.5 * (lo[1] + hi[1]),
                  gcz = 0.5 * (lo[2] + hi[2]);
+    {
+      float tx[kTPL], ty[kTPL], tz[kTPL];
 #pragma unroll
-    for (int q = 0; q < kTPL; ++q) {
-      T.tx[q] = (float)(tp[q].x - gcx);
-      T.ty[q] = (float)(tp[q].y - gcy);
-      T.tz[q] = (float)(tp[q].z - gcz);
+      for (int q = 0; q < kTPL; ++q) {
+        tx[q] = -(float)(tp[q].x - gcx);
+        ty[q] = -(float)(tp[q].y - gcy);
+        tz[q] = -(float)(tp[q].z - gcz);
+      }
+#pragma unroll
+      for (int q = 0; q < kTPL; ++q) {
+        T.ntx[q] = make_float2(tx[q], tx[q]);
+        T.nty[q] = make_float2(ty[q], ty[q]);
+        T.ntz[q] = make_float2(tz[q], tz[q]);
+      }
     }
     // a group's targets belong to one system: walk that system's subtree
     const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
     const int root = ws.root_pre[sys];
     const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
-    const float eps2 = (float)(soft * soft);
+    const float eps2f = (float)(soft * soft);
+    const float2 eps2 = make_float2(eps2f, eps2f);
     int ls = 0;
     if (lane == 0) stack[0] = root;
     int sp = (m > 0 && root >= 0 && root < m) ? 1 : 0;
@@ -422,7 +460,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
       const unsigned cm = __ballot_sync(kFull, cat == 1);
       if (cat == 1) {
         const int pos = ls + __popc(cm & lt);
-        list[pos] = make_float4((float)(a.x - gcx), (float)(a.y - gcy), (float)(a.z - gcz), (float)a.w);
+        list.put(pos, (float)(a.x - gcx), (float)(a.y - gcy), (float)(a.z - gcz), (float)a.w);
         if (kTrackSource) src[pos] = -1;
       }
       ls += __popc(cm);
@@ -438,7 +476,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
         for (int j = 0; j < lc; ++j) {
           const double4 q = ws.pm4[meta.y + j];
           const int pos = ls + linc - lc + j;
-          list[pos] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+          list.put(pos, (float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
           if (kTrackSource) src[pos] = meta.y + j;
         }
         ls += ltotal;
@@ -457,7 +495,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
             const int j = b0 + lane;
             if (j < cnt) {
               const double4 q = ws.pm4[first + j];
-              list[ls + lane] = make_float4((float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+              list.put(ls + lane, (float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
               if (kTrackSource) src[ls + lane] = first + j;
             }
             ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
@@ -468,6 +506,15 @@ __global__ void __launch_bounds__(kMixedWarps * 32, kTPL >= 4 ? NBB_MIXED_MINBLO
       }
     }
     if (ls > 0) {
+      if (ls & 1) {
+        // complete the last pair with a zero-mass entry far away (its
+        // offset squared stays finite in FP32 and it contributes exactly 0)
+        if (lane == 0) {
+          list.put(ls, 1.0e18f, 1.0e18f, 1.0e18f, 0.f);
+          if (kTrackSource) src[ls] = -2;
+        }
+        __syncwarp();
+      }
       const bool sg = eval_slots<kTrackSource, kTPL>(list, src, ls, nq, T, eps2);
 #pragma unroll
       for (int q = 0; q < kTPL; ++q)
