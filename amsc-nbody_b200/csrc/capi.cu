@@ -425,6 +425,7 @@ int nbb_selftest_bounded_wait(void) {
 
 int nbb_measure_fma_tflops(int precision, double *tflops) {
   if (!tflops) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
+  if (precision < 0 || precision > 2) return fail(NBB_ERR_INVALID_ARGUMENT, "precision must be 0, 1 or 2");
   NBB_CUDA(measure_fma_tflops(precision, tflops), "FMA throughput kernel");
   return ok();
 }

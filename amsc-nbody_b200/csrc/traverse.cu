@@ -795,6 +795,22 @@ __global__ void __launch_bounds__(256) fma_peak_kernel(T *out, int iters, T a, T
   if (s == (T)-12345) out[threadIdx.x] = s;
 }
 
+// Packed two-wide FP32 variant (sm_100 FFMA2): 8 independent float2 chains.
+__global__ void __launch_bounds__(256) fma2_peak_kernel(float *out, int iters, float a, float b) {
+  const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+  float2 x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = make_float2(threadIdx.x * 1e-3f + k, threadIdx.x * 1e-3f - k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = __ffma2_rn(x[k], a2, b2);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k].x + x[k].y;
+  if (s == -12345.f) out[threadIdx.x] = s;
+}
+
 inline int stream_grid(size_t n, int num_sms) {
   size_t b = (n + 255) / 256;
   const size_t cap = (size_t)(num_sms > 0 ? num_sms : 148) * 8;
@@ -863,8 +879,10 @@ cudaError_t measure_fma_tflops(int precision, double *tflops) {
     cudaEventRecord(e0);
     if (precision == 0)
       fma_peak_kernel<double><<<blocks, threads>>>((double *)out, iters, 0.9999999, 1e-9);
-    else
+    else if (precision == 1)
       fma_peak_kernel<float><<<blocks, threads>>>((float *)out, iters * 2, 0.9999f, 1e-6f);
+    else
+      fma2_peak_kernel<<<blocks, threads>>>((float *)out, iters, 0.9999f, 1e-6f);
     cudaEventRecord(e1);
     e = cudaEventSynchronize(e1);
     float ms = 0.f;
@@ -876,6 +894,7 @@ cudaError_t measure_fma_tflops(int precision, double *tflops) {
   cudaEventDestroy(e1);
   cudaFree(out);
   if (e != cudaSuccess) return e;
+  // FP64: iters x 8 FMAs; FP32: 2 iters x 8; packed: iters x 8 x 2 lanes
   const double flops = 2.0 * 8.0 * (double)iters * (precision == 0 ? 1.0 : 2.0) * blocks * threads;
   *tflops = flops / (best * 1e-3) / 1e12;
   return cudaSuccess;

@@ -238,8 +238,8 @@ int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right,
                    int *rfirst, int *rlast, int *plen, int *parent);
 
 /* Diagnostic: measured SIMT FMA throughput of the current device in TFLOP/s
- * (precision NBB_PRECISION_FP64 or NBB_PRECISION_MIXED = FP32), the
- * roofline denominator of the traversal kernels. */
+ * (precision NBB_PRECISION_FP64, NBB_PRECISION_MIXED = scalar FP32, or 2 =
+ * packed two-wide FP32), the roofline denominators of the traversal kernels. */
 int nbb_measure_fma_tflops(int precision, double *tflops);
 
 /* ------------------------------------------------- allocation-free ---- */
