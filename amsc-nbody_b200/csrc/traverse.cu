@@ -171,6 +171,7 @@ struct PairList {
 
 template <bool kTrackSource>
 struct MixedShared {
+  double gbox[kMixedWarps][9];  // group box lo (3), hi (3), centre (3)
   int stack[kMixedWarps][kStackCap];
   float4 la[kMixedWarps][kListCap / 2];
   float4 lb[kMixedWarps][kListCap / 2];
@@ -198,6 +199,11 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 // same FP64 difference -- and contributes exactly zero, so no source index is
 // needed.  With zero softening the source index excludes self and detects
 // the reference's singular interaction (returns true).
+#ifndef NBB_EVAL_UNROLL
+#define NBB_EVAL_UNROLL 4
+#endif
+constexpr int kEvalUnroll = NBB_EVAL_UNROLL;  // pairs per unrolled block of the evaluation loop
+
 template <bool kTrackSource, int kTPL>
 __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src, int count, const int *self,
                                            const float2 *ntx, const float2 *nty, const float2 *ntz, float2 eps2,
@@ -208,7 +214,7 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
   const float2 neg_half = make_float2(-0.5f, -0.5f), three_halves = make_float2(1.5f, 1.5f);
   bool singular = false;
   const int pairs = (count + 1) >> 1;
-#pragma unroll 4
+#pragma unroll kEvalUnroll
   for (int pr = 0; pr < pairs; ++pr) {
     const float4 ea = list.a[pr], eb = list.b[pr];
     const float2 ex = make_float2(ea.x, ea.y), ey = make_float2(ea.z, ea.w);
@@ -368,6 +374,20 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         hi[a] = fmax(hi[a], __shfl_xor_sync(kFull, hi[a], o));
       }
     }
+    {
+      // the box and centre live in shared memory while the walk runs, so
+      // they hold no registers through the evaluation
+      volatile double *gb = sh.gbox[wid];
+      if (lane == 0) {
+        for (int a = 0; a < 3; ++a) {
+          gb[a] = lo[a];
+          gb[3 + a] = hi[a];
+          gb[6 + a] = 0.5 * (lo[a] + hi[a]);
+        }
+      }
+      __syncwarp();
+    }
+    const volatile double *gbox = sh.gbox[wid];
     const double gcx = 0.5 * (lo[0] + hi[0]), gcy = 0.5 * (lo[1] + hi[1]),
                  gcz = 0.5 * (lo[2] + hi[2]);
     {
@@ -423,8 +443,9 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
           double d2 = 0.0;
 #pragma unroll
           for (int ax = 0; ax < 3; ++ax) {
-            overlap = overlap && hi[ax] >= cen[ax] - b.w && lo[ax] <= cen[ax] + b.w;
-            const double e = fmax(0.0, fmax(lo[ax] - com[ax], com[ax] - hi[ax]));
+            const double l = gbox[ax], h = gbox[3 + ax];
+            overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
+            const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
             d2 = fma(e, e, d2);
           }
           ++tests;
@@ -460,7 +481,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       const unsigned cm = __ballot_sync(kFull, cat == 1);
       if (cat == 1) {
         const int pos = ls + __popc(cm & lt);
-        list.put(pos, (float)(a.x - gcx), (float)(a.y - gcy), (float)(a.z - gcz), (float)a.w);
+        list.put(pos, (float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
         if (kTrackSource) src[pos] = -1;
       }
       ls += __popc(cm);
@@ -476,7 +497,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         for (int j = 0; j < lc; ++j) {
           const double4 q = ws.pm4[meta.y + j];
           const int pos = ls + linc - lc + j;
-          list.put(pos, (float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+          list.put(pos, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]), (float)q.w);
           if (kTrackSource) src[pos] = meta.y + j;
         }
         ls += ltotal;
@@ -495,7 +516,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
             const int j = b0 + lane;
             if (j < cnt) {
               const double4 q = ws.pm4[first + j];
-              list.put(ls + lane, (float)(q.x - gcx), (float)(q.y - gcy), (float)(q.z - gcz), (float)q.w);
+              list.put(ls + lane, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]), (float)q.w);
               if (kTrackSource) src[ls + lane] = first + j;
             }
             ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
