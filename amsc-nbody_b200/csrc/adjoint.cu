@@ -147,71 +147,75 @@ __global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, Travers
     if (grp >= n_groups) break;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
-    const int s = g0 + lane;
-    const bool valid = s < g1 && s < n;
-    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
-    double cx = 0.0, cy = 0.0, cz = 0.0;
-    if (valid) {
-      t = ws.pm4[s];
-      const uint32_t ti = ws.idx[s];
-      cx = ab.coef * ab.gvx[ti];
-      cy = ab.coef * ab.gvy[ti];
-      cz = ab.coef * ab.gvz[ti];
-    }
-    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
-    const int root = ws.root_pre[sys];
-    const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
-    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
-    const double soft2 = __dmul_rn(soft, soft);
-    double gtx = 0.0, gty = 0.0, gtz = 0.0;
-    int resume = valid ? root : INT_MAX;
-    int node = __reduce_min_sync(kFull, resume);
-    while (node < end) {
-      const int4 meta = ws.node_meta[node];
-      const double4 a = ws.node_a[node];
-      const bool here = resume == node;
-      if (meta.z > 0) {
-        for (int k = 0; k < meta.z; ++k) {
-          const int sp = meta.y + k;
-          const double4 q = ws.pm4[sp];
-          const bool act = here && sp != s && q.w != 0.0;
-          double ux = 0.0, uy = 0.0, uz = 0.0, uw = 0.0;
-          if (act) {
-            const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
-            singular |= !vjp_pair(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, cx, cy, cz, ux, uy, uz, uw);
-            gtx -= ux;
-            gty -= uy;
-            gtz -= uz;
-          }
-          const unsigned who = __ballot_sync(kFull, act);
-          if (who) scatter4(ab.part_g + sp, who, lane, ux, uy, uz, uw);
-        }
-        if (here) resume = meta.x;
-      } else if (a.w == 0.0) {
-        if (here) resume = meta.x;
-      } else {
-        const double4 c = ws.node_c[node];
-        const double4 b = ws.node_b[node];
-        bool acc = false;
-        double ux = 0.0, uy = 0.0, uz = 0.0, uw = 0.0;
-        if (here) {
-          double dx, dy, dz, d2;
-          acc = accept_fp64(a, b, c, t, dx, dy, dz, d2);
-          if (acc) {
-            singular |= !vjp_pair(dx, dy, dz, d2, a.w, g, soft2, cx, cy, cz, ux, uy, uz, uw);
-            gtx -= ux;
-            gty -= uy;
-            gtz -= uz;
-          }
-          resume = acc ? meta.x : node + 1;
-        }
-        const unsigned who = __ballot_sync(kFull, acc);
-        if (who) scatter4(ab.node_g + node, who, lane, ux, uy, uz, uw);
+    // a group larger than a warp is walked 32 targets at a time
+    for (int c0 = g0; c0 < g1; c0 += 32) {
+      const int c1 = min(c0 + 32, g1);
+      const int s = c0 + lane;
+      const bool valid = s < c1 && s < n;
+      double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+      double cx = 0.0, cy = 0.0, cz = 0.0;
+      if (valid) {
+        t = ws.pm4[s];
+        const uint32_t ti = ws.idx[s];
+        cx = ab.coef * ab.gvx[ti];
+        cy = ab.coef * ab.gvy[ti];
+        cz = ab.coef * ab.gvz[ti];
       }
-      if (resume <= node) resume = node + 1;
-      node = __reduce_min_sync(kFull, resume);
+      const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+      const int root = ws.root_pre[sys];
+      const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
+      const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+      const double soft2 = __dmul_rn(soft, soft);
+      double gtx = 0.0, gty = 0.0, gtz = 0.0;
+      int resume = valid ? root : INT_MAX;
+      int node = __reduce_min_sync(kFull, resume);
+      while (node < end) {
+        const int4 meta = ws.node_meta[node];
+        const double4 a = ws.node_a[node];
+        const bool here = resume == node;
+        if (meta.z > 0) {
+          for (int k = 0; k < meta.z; ++k) {
+            const int sp = meta.y + k;
+            const double4 q = ws.pm4[sp];
+            const bool act = here && sp != s && q.w != 0.0;
+            double ux = 0.0, uy = 0.0, uz = 0.0, uw = 0.0;
+            if (act) {
+              const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
+              singular |= !vjp_pair(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, cx, cy, cz, ux, uy, uz, uw);
+              gtx -= ux;
+              gty -= uy;
+              gtz -= uz;
+            }
+            const unsigned who = __ballot_sync(kFull, act);
+            if (who) scatter4(ab.part_g + sp, who, lane, ux, uy, uz, uw);
+          }
+          if (here) resume = meta.x;
+        } else if (a.w == 0.0) {
+          if (here) resume = meta.x;
+        } else {
+          const double4 c = ws.node_c[node];
+          const double4 b = ws.node_b[node];
+          bool acc = false;
+          double ux = 0.0, uy = 0.0, uz = 0.0, uw = 0.0;
+          if (here) {
+            double dx, dy, dz, d2;
+            acc = accept_fp64(a, b, c, t, dx, dy, dz, d2);
+            if (acc) {
+              singular |= !vjp_pair(dx, dy, dz, d2, a.w, g, soft2, cx, cy, cz, ux, uy, uz, uw);
+              gtx -= ux;
+              gty -= uy;
+              gtz -= uz;
+            }
+            resume = acc ? meta.x : node + 1;
+          }
+          const unsigned who = __ballot_sync(kFull, acc);
+          if (who) scatter4(ab.node_g + node, who, lane, ux, uy, uz, uw);
+        }
+        if (resume <= node) resume = node + 1;
+        node = __reduce_min_sync(kFull, resume);
+      }
+      if (valid) ab.tgt_g[s] = make_double4(gtx, gty, gtz, 0.0);
     }
-    if (valid) ab.tgt_g[s] = make_double4(gtx, gty, gtz, 0.0);
   }
   if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
 }
@@ -366,59 +370,63 @@ __global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, Traversa
     const double4 *node_aq = fb.node_aq + (size_t)q * cap;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
-    const int s = g0 + lane;
-    const bool valid = s < g1 && s < n;
-    double4 t = make_double4(0.0, 0.0, 0.0, 0.0), tq = t;
-    if (valid) {
-      t = ws.pm4[s];
-      tq = pm4q[s];
-    }
-    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
-    const int root = ws.root_pre[sys];
-    const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
-    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
-    const double soft2 = __dmul_rn(soft, soft);
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    int resume = valid ? root : INT_MAX;
-    int node = __reduce_min_sync(kFull, resume);
-    while (node < end) {
-      const int4 meta = ws.node_meta[node];
-      const double4 a = ws.node_a[node];
-      const double4 c = ws.node_c[node];
-      const double4 b = ws.node_b[node];
-      if (resume == node) {
-        if (meta.z > 0) {
-          for (int k = 0; k < meta.z; ++k) {
-            const int sp = meta.y + k;
-            if (sp == s) continue;
-            if (ws.pm4[sp].w == 0.0) continue;
-            const double4 u = pm4q[sp];
-            const double dx = __dsub_rn(u.x, tq.x), dy = __dsub_rn(u.y, tq.y), dz = __dsub_rn(u.z, tq.z);
-            singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), u.w, g, soft2, ax, ay, az);
-          }
-          resume = meta.x;
-        } else if (a.w == 0.0) {
-          resume = meta.x;
-        } else {
-          double dx, dy, dz, d2;
-          if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
-            const double4 aq = node_aq[node];
-            const double ex = __dsub_rn(aq.x, tq.x), ey = __dsub_rn(aq.y, tq.y), ez = __dsub_rn(aq.z, tq.z);
-            singular |= !point_mass_fp64(ex, ey, ez, sqdist(ex, ey, ez), aq.w, g, soft2, ax, ay, az);
+    // a group larger than a warp is walked 32 targets at a time
+    for (int c0 = g0; c0 < g1; c0 += 32) {
+      const int c1 = min(c0 + 32, g1);
+      const int s = c0 + lane;
+      const bool valid = s < c1 && s < n;
+      double4 t = make_double4(0.0, 0.0, 0.0, 0.0), tq = t;
+      if (valid) {
+        t = ws.pm4[s];
+        tq = pm4q[s];
+      }
+      const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+      const int root = ws.root_pre[sys];
+      const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
+      const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+      const double soft2 = __dmul_rn(soft, soft);
+      double ax = 0.0, ay = 0.0, az = 0.0;
+      int resume = valid ? root : INT_MAX;
+      int node = __reduce_min_sync(kFull, resume);
+      while (node < end) {
+        const int4 meta = ws.node_meta[node];
+        const double4 a = ws.node_a[node];
+        const double4 c = ws.node_c[node];
+        const double4 b = ws.node_b[node];
+        if (resume == node) {
+          if (meta.z > 0) {
+            for (int k = 0; k < meta.z; ++k) {
+              const int sp = meta.y + k;
+              if (sp == s) continue;
+              if (ws.pm4[sp].w == 0.0) continue;
+              const double4 u = pm4q[sp];
+              const double dx = __dsub_rn(u.x, tq.x), dy = __dsub_rn(u.y, tq.y), dz = __dsub_rn(u.z, tq.z);
+              singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), u.w, g, soft2, ax, ay, az);
+            }
+            resume = meta.x;
+          } else if (a.w == 0.0) {
             resume = meta.x;
           } else {
-            resume = node + 1;
+            double dx, dy, dz, d2;
+            if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
+              const double4 aq = node_aq[node];
+              const double ex = __dsub_rn(aq.x, tq.x), ey = __dsub_rn(aq.y, tq.y), ez = __dsub_rn(aq.z, tq.z);
+              singular |= !point_mass_fp64(ex, ey, ez, sqdist(ex, ey, ez), aq.w, g, soft2, ax, ay, az);
+              resume = meta.x;
+            } else {
+              resume = node + 1;
+            }
           }
         }
+        if (resume <= node) resume = node + 1;
+        node = __reduce_min_sync(kFull, resume);
       }
-      if (resume <= node) resume = node + 1;
-      node = __reduce_min_sync(kFull, resume);
-    }
-    if (valid) {
-      const size_t ti = (size_t)q * n + ws.idx[s];
-      fb.ax[ti] = ax;
-      fb.ay[ti] = ay;
-      fb.az[ti] = az;
+      if (valid) {
+        const size_t ti = (size_t)q * n + ws.idx[s];
+        fb.ax[ti] = ax;
+        fb.ay[ti] = ay;
+        fb.az[ti] = az;
+      }
     }
   }
   if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);

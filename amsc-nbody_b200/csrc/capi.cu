@@ -383,6 +383,7 @@ struct nbb_sim {
   cudaGraph_t step_graph_def = nullptr;
   uint64_t graph_kernels = 0;
   int tuned_group_size = 0;
+  int tuned_fp64_grouping = -1;  // plain walk: 0 Morton slices, 1 octree groups; -1 untuned
   double min_softening = 0.0;  // ensembles: smallest per-system softening
   std::unique_ptr<RolloutRecord> rollout;
   std::unique_ptr<FrameBuffers> frames;
@@ -557,6 +558,7 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size
                                           : (sim->tuned_group_size > 0 ? sim->tuned_group_size : 32);
   tp.group_mode = default_group_mode(tp.precision);
+  if (tp.precision == NBB_PRECISION_FP64 && sim->tuned_fp64_grouping >= 0) tp.group_mode = sim->tuned_fp64_grouping;
   if (sim->ws.n_systems > 1) {
     tp.group_mode = 1;  // a warp's targets must share a system
     tp.soft = sim->min_softening;
@@ -627,6 +629,60 @@ static int autotune_group_size(nbb_sim *sim) {
   return check_device(ws, sim->stream);
 }
 
+// Grouping autotuner of the plain FP64 walk: every lane follows its own
+// target's node sequence, so results do not depend on which targets share a
+// warp, only the time does -- fixed slices of 32 Morton-consecutive targets
+// (short runs, best for large systems) or octree target groups of at most 32
+// (compact, best where few warps must fill the GPU).  Timed on the tree of
+// the first force evaluation (best of two each), cached per process and
+// power-of-two size bucket.
+static std::vector<std::pair<int, int>> g_tuned_fp64;  // (log2 bucket, grouping)
+
+static int autotune_fp64_grouping(nbb_sim *sim) {
+  Workspace &ws = sim->ws;
+  int bucket = 0;
+  while ((1 << bucket) < ws.n && bucket < 31) ++bucket;
+  {
+    std::lock_guard<std::mutex> g(g_tune_lock);
+    for (const auto &kv : g_tuned_fp64)
+      if (kv.first == bucket) {
+        sim->tuned_fp64_grouping = kv.second;
+        return ok();
+      }
+  }
+  cudaStream_t s = sim->stream;
+  cudaEvent_t e0, e1;
+  NBB_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
+  NBB_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
+  float best = 1e30f;
+  int best_mode = 0;
+  cudaError_t e = cudaSuccess;
+  for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
+    TraversalParams tp = traversal_params(sim, 0);
+    tp.group_mode = mode;
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+      e = launch_retarget(ws, s);
+      if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e == cudaSuccess && ms < best) {
+        best = ms;
+        best_mode = mode;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(e, "walk grouping autotuning");
+  sim->tuned_fp64_grouping = best_mode;
+  std::lock_guard<std::mutex> g(g_tune_lock);
+  g_tuned_fp64.emplace_back(bucket, best_mode);
+  return check_device(ws, s);
+}
+
 int nbb_sim_initialize(nbb_sim *sim) {
   if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
   if (sim->state != nbb_sim::State::created)
@@ -645,6 +701,13 @@ int nbb_sim_initialize(nbb_sim *sim) {
   }
   if (sim->cfg.precision == NBB_PRECISION_MIXED && sim->cfg.group_size == 0) {
     st = autotune_group_size(sim);
+    if (st) {
+      sim->state = nbb_sim::State::failed;
+      return st;
+    }
+  }
+  if (sim->cfg.precision == NBB_PRECISION_FP64 && ws.n_systems == 1) {
+    st = autotune_fp64_grouping(sim);
     if (st) {
       sim->state = nbb_sim::State::failed;
       return st;
@@ -1131,11 +1194,14 @@ cudaError_t copy_state(nbb_sim *sim, double *slot, int count, bool save) {
 cudaError_t enqueue_vjp(nbb_sim *sim, const TraversalParams &tpa, const AdjointBuffers &ab) {
   Workspace &ws = sim->ws;
   cudaStream_t s = sim->stream;
+  const int group_max = ws.group_max;
+  ws.group_max = 32;  // target groups of one warp (kernels take the workspace by value)
   cudaError_t e = launch_step_reset(ws, s);
   if (e == cudaSuccess) e = launch_kd_bbox(ws, 0.0, 0, s);
   if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
   if (e == cudaSuccess) e = launch_tree(ws, tpa.theta, s);
   if (e == cudaSuccess) e = launch_adjoint_force(ws, tpa, ab, s);
+  ws.group_max = group_max;
   return e;
 }
 
@@ -1243,7 +1309,7 @@ int nbb_sim_backward(nbb_sim *sim, const double *gx, const double *gy, const dou
   TraversalParams tpa = traversal_params(sim, 0);
   tpa.precision = 0;
   tpa.kick = 0;
-  tpa.group_mode = ws.n_systems > 1 ? 1 : 0;
+  tpa.group_mode = 1;  // compact warps; the sums per interaction do not depend on it
   cudaError_t e = cudaSuccess;
   if (S > 0) {
     // the step s -> s+1 is undone by the VJP at x_{s+1} with accelerations
@@ -1529,12 +1595,15 @@ int nbb_sim_diagnostics(nbb_sim *sim, int potential, nbb_diagnostics *d) {
     // to other positions, e.g. after a backward pass)
     TraversalParams tp = traversal_params(sim, 0);
     tp.precision = 0;
-    tp.group_mode = ws.n_systems > 1 ? 1 : 0;
+    tp.group_mode = 1;
+    const int group_max = ws.group_max;
+    ws.group_max = 32;  // target groups of one warp
     cudaError_t e = launch_step_reset(ws, s);
     if (e == cudaSuccess) e = launch_kd_bbox(ws, 0.0, 0, s);
     if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
     if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
     if (e == cudaSuccess) e = launch_potential_tree(ws, tp, db.phi, s);
+    ws.group_max = group_max;
     NBB_CUDA(e, "potential evaluation");
     phi = db.phi;
   } else if (potential == NBB_POTENTIAL_DIRECT) {

@@ -98,52 +98,56 @@ __global__ void __launch_bounds__(256) potential_tree_kernel(Workspace ws, Trave
     if (grp >= n_groups) break;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
-    const int s = g0 + lane;
-    const bool valid = s < g1 && s < n;
-    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (valid) t = ws.pm4[s];
-    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
-    const int root = ws.root_pre[sys];
-    const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
-    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
-    const double soft2 = soft * soft;
-    double acc = 0.0;
-    int resume = valid ? root : INT_MAX;
-    int node = __reduce_min_sync(kFull, resume);
-    while (node < end) {
-      const int4 meta = ws.node_meta[node];
-      const double4 a = ws.node_a[node];
-      const double4 c = ws.node_c[node];
-      const double4 b = ws.node_b[node];
-      if (resume == node) {
-        if (meta.z > 0) {
-          for (int k = 0; k < meta.z; ++k) {
-            const int sp = meta.y + k;
-            if (sp == s) continue;
-            const double4 q = ws.pm4[sp];
-            if (q.w == 0.0) continue;
-            const double dx = q.x - t.x, dy = q.y - t.y, dz = q.z - t.z;
-            const double r2 = dx * dx + dy * dy + dz * dz + soft2;
-            if (r2 > 0.0) acc += q.w / sqrt(r2);
-          }
-          resume = meta.x;
-        } else if (a.w == 0.0) {
-          resume = meta.x;
-        } else {
-          double dx, dy, dz, d2;
-          if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
-            const double r2 = d2 + soft2;
-            if (r2 > 0.0) acc += a.w / sqrt(r2);
+    // a group larger than a warp is walked 32 targets at a time
+    for (int c0 = g0; c0 < g1; c0 += 32) {
+      const int c1 = min(c0 + 32, g1);
+      const int s = c0 + lane;
+      const bool valid = s < c1 && s < n;
+      double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (valid) t = ws.pm4[s];
+      const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+      const int root = ws.root_pre[sys];
+      const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
+      const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+      const double soft2 = soft * soft;
+      double acc = 0.0;
+      int resume = valid ? root : INT_MAX;
+      int node = __reduce_min_sync(kFull, resume);
+      while (node < end) {
+        const int4 meta = ws.node_meta[node];
+        const double4 a = ws.node_a[node];
+        const double4 c = ws.node_c[node];
+        const double4 b = ws.node_b[node];
+        if (resume == node) {
+          if (meta.z > 0) {
+            for (int k = 0; k < meta.z; ++k) {
+              const int sp = meta.y + k;
+              if (sp == s) continue;
+              const double4 q = ws.pm4[sp];
+              if (q.w == 0.0) continue;
+              const double dx = q.x - t.x, dy = q.y - t.y, dz = q.z - t.z;
+              const double r2 = dx * dx + dy * dy + dz * dz + soft2;
+              if (r2 > 0.0) acc += q.w / sqrt(r2);
+            }
+            resume = meta.x;
+          } else if (a.w == 0.0) {
             resume = meta.x;
           } else {
-            resume = node + 1;
+            double dx, dy, dz, d2;
+            if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
+              const double r2 = d2 + soft2;
+              if (r2 > 0.0) acc += a.w / sqrt(r2);
+              resume = meta.x;
+            } else {
+              resume = node + 1;
+            }
           }
         }
+        if (resume <= node) resume = node + 1;
+        node = __reduce_min_sync(kFull, resume);
       }
-      if (resume <= node) resume = node + 1;
-      node = __reduce_min_sync(kFull, resume);
+      if (valid) phi[ws.idx[s]] = -p.g * acc;
     }
-    if (valid) phi[ws.idx[s]] = -p.g * acc;
   }
 }
 

@@ -54,70 +54,74 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
     if (grp >= n_groups) break;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
-    const int s = g0 + lane;
-    const bool valid = s < g1 && s < n;
-    double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (valid) t = ws.pm4[s];
-    // a warp's targets belong to one system: walk that system's subtree
-    const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
-    const int root = ws.root_pre[sys];
-    const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
-    const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
-    const double soft2 = __dmul_rn(soft, soft);
-    double ax = 0.0, ay = 0.0, az = 0.0;
-    int resume = valid ? root : INT_MAX;
-    int node = __reduce_min_sync(kFull, resume);
-    while (node < end) {
-      // every record of the node in one round trip (warp-uniform address:
-      // one broadcast transaction each)
-      const int4 meta = ws.node_meta[node];
-      const double4 a = ws.node_a[node];
-      const double4 c = ws.node_c[node];
-      const double4 b = ws.node_b[node];
-      if (resume == node) {
-        if (meta.z > 0) {
-          // occupied leaf: exact sum over its particles, self excluded
-          // (barnes_hut.cu:226-277)
-          for (int k = 0; k < meta.z; ++k) {
-            const int sp = meta.y + k;
-            if (sp == s) continue;
-            const double4 q = ws.pm4[sp];
-            if (q.w == 0.0) continue;
-            const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
-            singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
-            ++inter;
-          }
-          resume = meta.x;
-        } else if (a.w == 0.0) {
-          resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
-        } else {
-          double dx, dy, dz, d2;
-          const bool accept = accept_fp64(a, b, c, t, dx, dy, dz, d2);
-          ++tests;
-          if (accept) {
-            singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
-            ++inter;
+    // a group larger than a warp is walked 32 targets at a time
+    for (int c0 = g0; c0 < g1; c0 += 32) {
+      const int c1 = min(c0 + 32, g1);
+      const int s = c0 + lane;
+      const bool valid = s < c1 && s < n;
+      double4 t = make_double4(0.0, 0.0, 0.0, 0.0);
+      if (valid) t = ws.pm4[s];
+      // a warp's targets belong to one system: walk that system's subtree
+      const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
+      const int root = ws.root_pre[sys];
+      const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
+      const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
+      const double soft2 = __dmul_rn(soft, soft);
+      double ax = 0.0, ay = 0.0, az = 0.0;
+      int resume = valid ? root : INT_MAX;
+      int node = __reduce_min_sync(kFull, resume);
+      while (node < end) {
+        // every record of the node in one round trip (warp-uniform address:
+        // one broadcast transaction each)
+        const int4 meta = ws.node_meta[node];
+        const double4 a = ws.node_a[node];
+        const double4 c = ws.node_c[node];
+        const double4 b = ws.node_b[node];
+        if (resume == node) {
+          if (meta.z > 0) {
+            // occupied leaf: exact sum over its particles, self excluded
+            // (barnes_hut.cu:226-277)
+            for (int k = 0; k < meta.z; ++k) {
+              const int sp = meta.y + k;
+              if (sp == s) continue;
+              const double4 q = ws.pm4[sp];
+              if (q.w == 0.0) continue;
+              const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
+              singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
+              ++inter;
+            }
             resume = meta.x;
+          } else if (a.w == 0.0) {
+            resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
           } else {
-            resume = node + 1;
+            double dx, dy, dz, d2;
+            const bool accept = accept_fp64(a, b, c, t, dx, dy, dz, d2);
+            ++tests;
+            if (accept) {
+              singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
+              ++inter;
+              resume = meta.x;
+            } else {
+              resume = node + 1;
+            }
           }
         }
+        // a lane's resume index always moves forward (skip > node); this keeps
+        // the walk finite whatever the node records hold
+        if (resume <= node) resume = node + 1;
+        node = __reduce_min_sync(kFull, resume);
       }
-      // a lane's resume index always moves forward (skip > node); this keeps
-      // the walk finite whatever the node records hold
-      if (resume <= node) resume = node + 1;
-      node = __reduce_min_sync(kFull, resume);
-    }
-    if (valid) {
-      const uint32_t ti = ws.idx[s];
-      ws.ax[ti] = ax;
-      ws.ay[ti] = ay;
-      ws.az[ti] = az;
-      if (p.kick) {
-        // second half kick, integrator.cu:92-112
-        ws.vx[ti] = __fma_rn(p.half_dt, ax, ws.vx[ti]);
-        ws.vy[ti] = __fma_rn(p.half_dt, ay, ws.vy[ti]);
-        ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
+      if (valid) {
+        const uint32_t ti = ws.idx[s];
+        ws.ax[ti] = ax;
+        ws.ay[ti] = ay;
+        ws.az[ti] = az;
+        if (p.kick) {
+          // second half kick, integrator.cu:92-112
+          ws.vx[ti] = __fma_rn(p.half_dt, ax, ws.vx[ti]);
+          ws.vy[ti] = __fma_rn(p.half_dt, ay, ws.vy[ti]);
+          ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
+        }
       }
     }
   }
