@@ -172,13 +172,17 @@ def test_backward_restores_state_and_is_repeatable(nbb_mod, precision):
     assert np.array_equal(np.stack(sim.download()), np.stack(ref.download()))
 
 
-def test_mixed_rollout_gradient_close_to_fp64_gradient(nbb_mod):
+@pytest.mark.parametrize("group_size", [0, 32, 64, 128])
+def test_mixed_rollout_gradient_close_to_fp64_gradient(nbb_mod, group_size):
+    # the backward pass rebuilds one-warp target groups whatever group size
+    # the mixed walk uses
     n = 4096
     p = _plummer(nbb_mod, n, 19)
     wx, wv = _linear_loss_weights(n, 20)
     out = []
     for prec in (0, 1):
-        sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec))
+        sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec,
+                                                             group_size=group_size if prec else 0))
         sim.initialize()
         sim.rollout(12, 4)
         out.append(sim.backward(wx, wv))

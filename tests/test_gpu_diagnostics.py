@@ -91,3 +91,15 @@ def test_ensemble_diagnostics(nbb_mod):
     assert d["potential_energy"] < 0.0
     with pytest.raises(nbb_mod.InvalidArgument):
         sim.diagnostics(nbb_mod.POTENTIAL_DIRECT)
+
+
+@pytest.mark.parametrize("group_size", [32, 64, 128])
+def test_tree_potential_of_a_mixed_simulation(nbb_mod, group_size):
+    from nbb import ics
+
+    p = ics.plummer(3000, seed=45)
+    w = _direct_potential(p, 1.0, 0.01)
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.0, 0.01, 1.0, precision=nbb_mod.PRECISION_MIXED,
+                                                         group_size=group_size))
+    sim.initialize()
+    assert np.isclose(sim.diagnostics(nbb_mod.POTENTIAL_TREE)["potential_energy"], w, rtol=1e-12)
