@@ -477,9 +477,9 @@ def run_reference(args, rank, world, local):
                        "implementation": "reference CUDA sources (unmodified) built for sm_100a, "
                                          "Simulation::step order, per-step allocation and host "
                                          "syncs as in the reference"},
-            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 0, "kind": "reference",
-                             "sample": f"{steps} reference steps on the GPU (the reference has no "
-                                       "CPU implementation of the path)"},
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": 1, "kind": "reference",
+                             "sample": f"{steps} reference steps on the GPU, driven by one host "
+                                       "thread (the reference has no CPU implementation of the path)"},
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "clocks": sampler.summary()}
