@@ -1367,23 +1367,31 @@ cudaError_t launch_kd_bbox(Workspace &ws, double dt, int do_kd, cudaStream_t s) 
   return cudaGetLastError();
 }
 
-cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s) {
-  int blocks = (ws.n + kBlock - 1) / kBlock;
-  const int cap = grid_for(ws, 4);
-  if (blocks > cap) blocks = cap;
-  if (blocks < 1) blocks = 1;
-  encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
-  unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
-  for (int p = 0; p < ws.sort_passes; ++p) {
-    onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
-        src, dst, ws.n, p, ws.pack_shift + 8 * p, ws.digit_hist,
-        ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
-    unsigned long long *t = src;
-    src = dst;
-    dst = t;
+cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part) {
+  // the passes alternate between the two pair buffers
+  unsigned long long *sorted = (ws.sort_passes & 1) ? ws.pairs_b : ws.pairs_a;
+  if (part != 2) {
+    int blocks = (ws.n + kBlock - 1) / kBlock;
+    const int cap = grid_for(ws, 4);
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    encode_kernel<<<blocks, kBlock, 0, s>>>(ws);
+    unsigned long long *src = ws.pairs_a, *dst = ws.pairs_b;
+    for (int p = 0; p < ws.sort_passes; ++p) {
+      onesweep_kernel<<<ws.sort_tiles, kSortThreads, 0, s>>>(
+          src, dst, ws.n, p, ws.pack_shift + 8 * p, ws.digit_hist,
+          ws.sort_status + (size_t)p * ws.sort_tiles * 256, ws.sc);
+      unsigned long long *t = src;
+      src = dst;
+      dst = t;
+    }
+    count_launches(1 + ws.sort_passes);
   }
-  groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, src, 1);
-  count_launches(2 + ws.sort_passes);
+  if (part != 1) {
+    // the first reader of the masses (gathered with the sorted positions)
+    groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, sorted, 1);
+    count_launches(1);
+  }
   return cudaGetLastError();
 }
 

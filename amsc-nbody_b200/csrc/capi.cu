@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -309,12 +310,20 @@ int check_device(const Workspace &ws, cudaStream_t s) {
 
 // Rebuild + force on the workspace state (kd: first half kick + drift before
 // the rebuild; kick: second half kick fused into the traversal).
+// part: 0 the whole step; or one of its three parts: 1 reset and
+// kick-drift + box (the last writes of the positions), 2 Morton encode and
+// sort, 3 leaf groups with the gather (the first read of the masses), tree,
+// walk + kick.
 cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, double dt, int kd,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, int part = 0) {
   ws.group_max = (tp.group_mode && tp.group_size > 32) ? (tp.group_size > 64 ? 128 : 64) : 32;
-  cudaError_t e = launch_step_reset(ws, s);
-  if (e == cudaSuccess) e = launch_kd_bbox(ws, dt, kd, s);
-  if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
+  cudaError_t e = cudaSuccess;
+  if (part == 0 || part == 1) {
+    e = launch_step_reset(ws, s);
+    if (e == cudaSuccess) e = launch_kd_bbox(ws, dt, kd, s);
+  }
+  if (e == cudaSuccess && part != 1) e = launch_morton_sort_groups(ws, s, part == 0 ? 0 : part - 1);
+  if (part == 1 || part == 2) return e;
   if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
   if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
   return e;
@@ -363,6 +372,30 @@ struct FrameBuffers {
   FrameScalars *scalars = nullptr;
 };
 
+// A step with host state in and out (nbb_sim_step_host): the step split
+// into three graphs (enqueue_rebuild_force's parts) so that a second stream
+// uploads the masses while the positions are sorted and copies the drifted
+// positions to the host while the tree is rebuilt and walked.  Taken at the
+// first such step.
+struct HostStep {
+  static constexpr int kParts = 3;
+  cudaGraphExec_t exec[kParts] = {};
+  cudaGraph_t def[kParts] = {};
+  uint64_t kernels[kParts] = {};
+  cudaStream_t copy = nullptr;
+  cudaEvent_t state_in = nullptr, mass_in = nullptr, drifted = nullptr, copied = nullptr;
+  ~HostStep() {
+    if (copy) cudaStreamSynchronize(copy);
+    for (int k = 0; k < kParts; ++k) {
+      if (exec[k]) cudaGraphExecDestroy(exec[k]);
+      if (def[k]) cudaGraphDestroy(def[k]);
+    }
+    for (cudaEvent_t ev : {state_in, mass_in, drifted, copied})
+      if (ev) cudaEventDestroy(ev);
+    if (copy) cudaStreamDestroy(copy);
+  }
+};
+
 // Device buffers of the conserved-quantity monitor, taken at its first use.
 struct DiagBuffers {
   static constexpr int kBlocks = 592;  // fixed: the sums' order never changes
@@ -388,6 +421,7 @@ struct nbb_sim {
   std::unique_ptr<RolloutRecord> rollout;
   std::unique_ptr<FrameBuffers> frames;
   std::unique_ptr<DiagBuffers> diag;
+  std::unique_ptr<HostStep> host_step;
 };
 
 extern "C" {
@@ -781,6 +815,109 @@ int nbb_sim_run(nbb_sim *sim, uint64_t steps) {
   return run_steps(sim, steps, "Simulation must be initialized before running");
 }
 
+// Capture one part (1..3) of the step into a graph.
+static cudaError_t capture_part(nbb_sim *sim, int part, cudaGraph_t &def, cudaGraphExec_t &exec,
+                                uint64_t &kernels) {
+  const uint64_t before = nbb::launch_count();
+  cudaError_t e = cudaStreamBeginCapture(sim->own_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t body =
+      enqueue_rebuild_force(sim->ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->own_stream, part);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(sim->own_stream, &graph);
+  kernels = nbb::launch_count() - before;
+  nbb::count_launches((uint64_t)0 - kernels);
+  if (body != cudaSuccess || e != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return body != cudaSuccess ? body : e;
+  }
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return e;
+  }
+  def = graph;
+  return cudaSuccess;
+}
+
+static cudaError_t host_step_setup(nbb_sim *sim) {
+  if (sim->host_step) return cudaSuccess;
+  auto hs = std::make_unique<HostStep>();
+  cudaError_t e = cudaStreamCreateWithFlags(&hs->copy, cudaStreamNonBlocking);
+  for (cudaEvent_t *ev : {&hs->state_in, &hs->mass_in, &hs->drifted, &hs->copied})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  for (int k = 0; k < HostStep::kParts && e == cudaSuccess && sim->cfg.use_graph; ++k)
+    e = capture_part(sim, k + 1, hs->def[k], hs->exec[k], hs->kernels[k]);
+  if (e == cudaSuccess) sim->host_step = std::move(hs);
+  return e;
+}
+
+static cudaError_t enqueue_part(nbb_sim *sim, int part) {
+  HostStep &hs = *sim->host_step;
+  if (hs.exec[part - 1]) {
+    nbb::count_launches(hs.kernels[part - 1]);
+    return cudaGraphLaunch(hs.exec[part - 1], sim->stream);
+  }
+  return enqueue_rebuild_force(sim->ws, traversal_params(sim, 1), sim->cfg.time_step, 1, sim->stream, part);
+}
+
+int nbb_sim_step_host(nbb_sim *sim, const double *mass, const double *x, const double *y, const double *z,
+                      const double *vx, const double *vy, const double *vz, double *out_x, double *out_y,
+                      double *out_z, double *out_vx, double *out_vy, double *out_vz) {
+  if (!sim) return fail(NBB_ERR_INVALID_ARGUMENT, "null simulation");
+  if (sim->state != nbb_sim::State::ready)
+    return fail(NBB_ERR_LOGIC, "Simulation must be initialized before stepping");
+  NBB_CUDA(cudaSetDevice(sim->cfg.device), "cudaSetDevice");
+  Workspace &ws = sim->ws;
+  const size_t bytes = (size_t)ws.n * sizeof(double);
+  cudaError_t e = host_step_setup(sim);
+  if (e != cudaSuccess) return cuda_fail(e, "host step setup");
+  HostStep &hs = *sim->host_step;
+  cudaStream_t s = sim->stream;
+  // positions and velocities first: the kick-drift needs them
+  const double *src[6] = {x, y, z, vx, vy, vz};
+  double *dev[6] = {ws.x, ws.y, ws.z, ws.vx, ws.vy, ws.vz};
+  for (int k = 0; k < 6 && e == cudaSuccess; ++k)
+    if (src[k]) e = cudaMemcpyAsync(dev[k], src[k], bytes, cudaMemcpyHostToDevice, s);
+  // the masses follow on the second stream, under the kick-drift and sort
+  if (e == cudaSuccess) e = cudaEventRecord(hs.state_in, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(hs.copy, hs.state_in, 0);
+  if (e == cudaSuccess && mass) e = cudaMemcpyAsync(ws.m, mass, bytes, cudaMemcpyHostToDevice, hs.copy);
+  if (e == cudaSuccess) e = cudaEventRecord(hs.mass_in, hs.copy);
+  if (e == cudaSuccess) e = enqueue_part(sim, 1);
+  if (e == cudaSuccess) e = cudaEventRecord(hs.drifted, s);
+  if (e == cudaSuccess) e = enqueue_part(sim, 2);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, hs.mass_in, 0);
+  // the rest is queued before the positions' copy: a copy to pageable
+  // memory returns only when it is done
+  if (e == cudaSuccess) e = enqueue_part(sim, 3);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(hs.copy, hs.drifted, 0);
+  double *pos[3] = {out_x, out_y, out_z};
+  const double *dpos[3] = {ws.x, ws.y, ws.z};
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+    if (pos[k]) e = cudaMemcpyAsync(pos[k], dpos[k], bytes, cudaMemcpyDeviceToHost, hs.copy);
+  if (e == cudaSuccess) e = cudaEventRecord(hs.copied, hs.copy);
+  double *vel[3] = {out_vx, out_vy, out_vz};
+  const double *dvel[3] = {ws.vx, ws.vy, ws.vz};
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+    if (vel[k]) e = cudaMemcpyAsync(vel[k], dvel[k], bytes, cudaMemcpyDeviceToHost, s);
+  // the handle's stream ends after both streams' copies
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, hs.copied, 0);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(hs.copy);
+    sim->state = nbb_sim::State::failed;
+    return cuda_fail(e, "host step");
+  }
+  const int st = check_device(ws, s);
+  if (st) {
+    sim->state = nbb_sim::State::failed;
+    return st;
+  }
+  sim->time += sim->cfg.time_step;
+  sim->steps += 1;
+  return ok();
+}
+
 double nbb_sim_time(const nbb_sim *sim) { return sim ? sim->time : 0.0; }
 uint64_t nbb_sim_step_number(const nbb_sim *sim) { return sim ? sim->steps : 0; }
 
@@ -849,6 +986,7 @@ int nbb_sim_destroy(nbb_sim *sim) {
   if (sim->stream) cudaStreamSynchronize(sim->stream);
   if (sim->step_graph) cudaGraphExecDestroy(sim->step_graph);
   if (sim->step_graph_def) cudaGraphDestroy(sim->step_graph_def);
+  sim->host_step.reset();
   cudaStream_t s = sim->own_stream;
   delete sim;  // frees every device buffer
   if (s) cudaStreamDestroy(s);

@@ -241,7 +241,8 @@ cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s);
 // Kick-drift (optional) fused with the global bounding-box reduction.
 cudaError_t launch_kd_bbox(Workspace &ws, double dt, int do_kd, cudaStream_t s);
 // Morton encode + digit histograms, onesweep sort, groups + gather.
-cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s);
+// part: 0 all, 1 Morton encode + sort only, 2 leaf groups + gather only
+cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part = 0);
 // Karras tree, plan + scan, octree materialisation, geometry, physics,
 // preorder layout.
 cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s);

@@ -84,6 +84,7 @@ SIGNATURES = {
     "nbb_sim_upload": (_I, [_P] * 8),
     "nbb_sim_download": (_I, [_P] * 7),
     "nbb_sim_download_accel": (_I, [_P] * 4),
+    "nbb_sim_step_host": (_I, [_P] * 14),
     "nbb_sim_set_stream": (_I, [_P, _P]),
     "nbb_sim_synchronize": (_I, [_P]),
     "nbb_sim_destroy": (_I, [_P]),

@@ -128,6 +128,19 @@ class Simulation:
         check(self._lib.nbb_sim_download(self._handle, *[ptr(a) for a in out]))
         return out
 
+    def step_host(self, p: ParticleData | None = None, *, mass=None, x=None, y=None, z=None, vx=None,
+                  vy=None, vz=None, out=None):
+        """One step with host state in and out (upload + step + download in
+        one call, the positions' copy overlapping the walk).  Returns ``out``
+        (6 float64 arrays: x y z vx vy vz; new arrays when None)."""
+        if p is not None:
+            mass, x, y, z, vx, vy, vz = p.arrays()
+        if out is None:
+            out = [np.empty(self._n) for _ in range(6)]
+        check(self._lib.nbb_sim_step_host(self._handle, *[ptr(a) for a in (mass, x, y, z, vx, vy, vz)],
+                                          *[ptr(a) for a in out]))
+        return out
+
     def accelerations(self):
         """Current accelerations copied to host."""
         out = [np.empty(self._n) for _ in range(3)]

@@ -269,9 +269,10 @@ def run_nbb(args, rank, world, local):
         with torch.cuda.stream(stream):
             flush.zero_()
             e0.record(stream)
-        sim.upload(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6])
-        sim.step()
-        sim.download(out=hst[1:])
+        # upload, step and download in one call; the positions' copy back
+        # overlaps the rebuild and the walk
+        sim.step_host(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6],
+                      out=hst[1:])
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()

@@ -129,6 +129,24 @@ int nbb_sim_download(nbb_sim *sim, double *x, double *y, double *z,
 /* Accelerations of the current state to host memory. */
 int nbb_sim_download_accel(nbb_sim *sim, double *ax, double *ay, double *az);
 
+/* One step with the state in host memory: nbb_sim_upload + nbb_sim_step +
+ * nbb_sim_download in one call, with the same result bit for bit.  The
+ * reference copies host buffers to the device only when it loads particles
+ * (thrust::copy per block, src/particle.hpp:172-192) and hands out device
+ * views after that (Simulation::particles, src/simulation.cpp:133-134);
+ * this call serves a host that owns the state between steps.  Any input may
+ * be NULL (that array is not uploaded), and so may any output.  The masses
+ * are first read after the sort, so their upload overlaps the kick-drift
+ * and the sort on a second stream; the positions are final after the drift,
+ * so their copy to the host overlaps the rebuild and the walk; the
+ * velocities follow the closing kick.  Returns when every copy is
+ * complete. */
+int nbb_sim_step_host(nbb_sim *sim, const double *mass, const double *x,
+                      const double *y, const double *z, const double *vx,
+                      const double *vy, const double *vz, double *out_x,
+                      double *out_y, double *out_z, double *out_vx,
+                      double *out_vy, double *out_vz);
+
 /* Stream control: all work of the handle goes to this stream (a
  * cudaStream_t; NULL = the handle's own stream). */
 int nbb_sim_set_stream(nbb_sim *sim, void *stream);

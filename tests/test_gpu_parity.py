@@ -280,6 +280,50 @@ def test_graph_replay_equals_eager(nbb_mod, precision):
         assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("precision,graph", [(0, True), (1, True), (1, False)])
+def test_host_step_equals_upload_step_download(nbb_mod, precision, graph):
+    import torch
+    from nbb import ics
+
+    p = ics.plummer(30000, seed=5)
+    cfg = nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=precision, use_graph=graph)
+    a = nbb_mod.Simulation(p, cfg)
+    b = nbb_mod.Simulation(p, cfg)
+    with pytest.raises(nbb_mod.LogicError):
+        b.step_host(p)
+    a.initialize()
+    b.initialize()
+    state = [np.array(v) for v in p.arrays()[1:]]
+    pinned = [torch.from_numpy(v.copy()).pin_memory() for v in state]
+    for k in range(3):
+        # mass goes up on the first step only; the pinned copy on the last
+        mass = p.mass if k == 0 else None
+        a.upload(mass=mass, x=state[0], y=state[1], z=state[2], vx=state[3], vy=state[4], vz=state[5])
+        a.step()
+        want = a.download()
+        if k < 2:
+            got = b.step_host(mass=mass, x=state[0], y=state[1], z=state[2], vx=state[3], vy=state[4],
+                              vz=state[5])
+        else:
+            for t, v in zip(pinned, state):
+                t.copy_(torch.from_numpy(v))
+            b.step_host(x=pinned[0], y=pinned[1], z=pinned[2], vx=pinned[3], vy=pinned[4], vz=pinned[5],
+                        out=pinned)
+            got = [t.numpy() for t in pinned]
+        for w, g in zip(want, got):
+            assert np.array_equal(w, g)
+        state = [np.array(w) for w in want]
+    assert b.step_number() == a.step_number() == 3
+    assert b.time() == a.time()
+    # outputs may be left out; the device state still advances
+    b.step_host(x=state[0], y=state[1], z=state[2], vx=state[3], vy=state[4], vz=state[5],
+                out=[None] * 6)
+    a.upload(x=state[0], y=state[1], z=state[2], vx=state[3], vy=state[4], vz=state[5])
+    a.step()
+    for w, g in zip(a.download(), b.download()):
+        assert np.array_equal(w, g)
+
+
 def test_simulation_state_machine(nbb_mod):
     p = _particles([1.0, 1.0], [0.0, 1.0], [0.0, 0.0], [0.0, 0.0])
     cfg = nbb_mod.SimulationConfig(0.25, 0.5, 0.01, 1.0)
