@@ -311,6 +311,22 @@ __device__ __forceinline__ void flush_full(const PairList &list, int *src, int &
   }
 }
 
+// Exclusive prefix sum over the warp of a small count v in [0, 2^kBits):
+// one ballot per bit, no chain of dependent shuffles.  `total` receives the
+// warp's sum.
+template <int kBits>
+__device__ __forceinline__ int warp_prefix_small(int v, unsigned lt, int &total) {
+  int excl = 0;
+  total = 0;
+#pragma unroll
+  for (int b = 0; b < kBits; ++b) {
+    const unsigned m = __ballot_sync(kFull, (v >> b) & 1);
+    excl += __popc(m & lt) << b;
+    total += __popc(m) << b;
+  }
+  return excl;
+}
+
 // Mixed-precision traversal, one warp per target group of at most 32 x kTPL
 // Morton-consecutive targets inside one parent cell (kTPL targets per lane).
 // The group's bounding box (FP64) replaces the target in the reference's
@@ -458,20 +474,21 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       }
       // opened nodes push their children; a push that would not fit the
       // stack accepts the node instead (bounded walk, counted)
-      int nch = (cat == 3) ? meta.w : 0;
-      int incl = nch;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += v;
+      // (a node has at most 8 children: four bits per count)
+      int nch = (cat == 3) ? min(max(meta.w, 0), 8) : 0;
+      int all_children;
+      const int excl = warp_prefix_small<4>(nch, lt, all_children);
+      int pushed = all_children;
+      if (sp + all_children > kStackCap) {
+        // the lanes whose children would end past the stack's end accept
+        // their node instead; the pushes before them stand
+        if (nch > 0 && sp + excl + nch > kStackCap) {
+          cat = 1;
+          nch = 0;
+          ++overflow;
+        }
+        pushed = __reduce_max_sync(kFull, nch > 0 ? excl + nch : 0);
       }
-      const int excl = incl - nch;
-      if (nch > 0 && sp + incl > kStackCap) {
-        cat = 1;
-        nch = 0;
-        ++overflow;
-      }
-      int pushed = (nch > 0) ? incl : 0;
-      for (int o = 16; o > 0; o >>= 1) pushed = max(pushed, __shfl_xor_sync(kFull, pushed, o));
       if (nch > 0) {
         // children always follow their parent in preorder; anything else is
         // dropped so the walk stays finite
@@ -491,12 +508,17 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       ls += __popc(cm);
       // reached leaves -> their particles: all at once when they fit
       const int lc = (cat == 2) ? meta.z : 0;
-      int linc = lc;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(kFull, linc, o);
-        if (lane >= o) linc += v;
+      int linc, ltotal;
+      if (__all_sync(kFull, lc < 16)) {
+        linc = warp_prefix_small<4>(lc, lt, ltotal) + lc;
+      } else {
+        linc = lc;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(kFull, linc, o);
+          if (lane >= o) linc += v;
+        }
+        ltotal = __shfl_sync(kFull, linc, 31);
       }
-      const int ltotal = __shfl_sync(kFull, linc, 31);
       if (ls + ltotal <= kListCap) {
         for (int j = 0; j < lc; ++j) {
           const double4 q = ws.pm4[meta.y + j];
