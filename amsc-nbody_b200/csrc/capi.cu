@@ -225,7 +225,9 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   if (e != cudaSuccess) return e;
   e = cudaMemset(ws.root_pre, 0, S * sizeof(int));
   if (e != cudaSuccess) return e;
-  return configure_traversal(ws);
+  e = configure_traversal(ws);
+  if (e != cudaSuccess) return e;
+  return al.get(ws.walk_ext, (size_t)ws.walk_warps * ws.walk_ext_cap);
 }
 
 bool finite_nonneg(double v) { return std::isfinite(v) && v >= 0.0; }
@@ -1003,6 +1005,7 @@ int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats) {
   stats->interactions = (int64_t)sc.interactions;
   stats->mac_tests = (int64_t)sc.mac_tests;
   stats->group_size = sim->cfg.precision == NBB_PRECISION_MIXED ? traversal_params(sim, 0).group_size : 0;
+  stats->stack_overflow = (int64_t)sc.stack_overflow;
   return ok();
 }
 
@@ -1111,6 +1114,7 @@ int nbb_accel(size_t n, const double *mass, const double *x, const double *y, co
     stats->interactions = (int64_t)d.interactions;
     stats->mac_tests = (int64_t)d.mac_tests;
     stats->group_size = precision == NBB_PRECISION_MIXED ? tp.group_size : 0;
+    stats->stack_overflow = (int64_t)d.stack_overflow;
   }
   if (export_out) {
     st = export_workspace(ws, export_out, sc.s, true);

@@ -83,6 +83,8 @@ struct Workspace {
   int num_sms = 0;
   int fp64_grid = 0;    // persistent traversal grids (blocks)
   int mixed_grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // [track source][1, 2 or 4 targets per lane]
+  int walk_warps = 0;     // warps of the largest mixed-walk grid
+  int walk_ext_cap = 0;   // entries per warp of the mixed walk's stack extension
   int group_max = 32;   // largest octree target group: 32, 64 or 128 (32 x target slots per lane)
 
   // key layout: an ensemble's system id sits above the 30 Morton bits and
@@ -156,6 +158,7 @@ struct Workspace {
   double4 *node_c = nullptr;  // crit, crit^2 lower/upper band, unused
   int4 *node_meta = nullptr;  // skip, first particle, particle count, nchild
   int *node_kids = nullptr;   // 8 per node, preorder ids in visit order
+  int *walk_ext = nullptr;    // walk_warps x walk_ext_cap: the mixed walk's stack below shared memory
 };
 
 // ------------------------------------------------------------ helpers ---

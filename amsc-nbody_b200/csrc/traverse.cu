@@ -13,6 +13,7 @@
 #include "nbb_internal.cuh"
 #include "walk_fp64.cuh"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -142,19 +143,21 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
 #define NBB_MIXED_WARPS 2
 #endif
 #ifndef NBB_MIXED_MINBLOCKS
-#define NBB_MIXED_MINBLOCKS 12
+#define NBB_MIXED_MINBLOCKS 10
 #endif
 // resident blocks per SM for the two- and four-targets-per-lane instances
 // (more registers per thread for the targets' sums)
 #ifndef NBB_MIXED_MINBLOCKS2
-#define NBB_MIXED_MINBLOCKS2 10
+#define NBB_MIXED_MINBLOCKS2 8
 #endif
 #ifndef NBB_MIXED_MINBLOCKS4
-#define NBB_MIXED_MINBLOCKS4 8
+#define NBB_MIXED_MINBLOCKS4 7
 #endif
 constexpr int kMixedWarps = NBB_MIXED_WARPS;
-constexpr int kStackCap = 512;
-constexpr int kListCap = 96;
+constexpr int kWalkPop = 64;     // nodes per round: two per lane
+constexpr int kStackCap = 1024;  // shared-memory part of a warp's stack
+constexpr int kSpill = 512;      // entries moved to / from the global extension at once
+constexpr int kListCap = 192;    // < 32 left over + 64 cells + up to 96 leaf particles
 
 // The interaction list keeps entries in pairs so that packed two-wide FP32
 // instructions (sm_100's FADD2 / FMUL2 / FFMA2) evaluate two entries at once
@@ -333,12 +336,13 @@ __device__ __forceinline__ int warp_prefix_small(int v, unsigned lt, int &total)
 // acceptance test: a node is accepted for the whole group when the box does
 // not touch the cell and the box-to-centre-of-mass distance exceeds
 // crit = side/theta + |com - centre|, which implies acceptance for every
-// target in the box.  Nodes are examined 32 at a time (one per lane) from a
-// warp-private stack in shared memory, each lane fetching its node's record
-// and child list in one round trip; accepted nodes and the particles of
-// reached leaves go to a shared interaction list as FP32 offsets from the
-// group centre (formed in FP64, then rounded) and are evaluated by all lanes
-// in batches of 32.
+// target in the box.  Nodes are examined 64 at a time (two per lane) from a
+// warp-private stack in shared memory, each lane fetching both nodes'
+// records and child lists in one round trip; a full stack spills its bottom
+// half to a global extension sized for any walk, so every node gets the
+// acceptance test.  Accepted nodes and the particles of reached leaves go to
+// a shared interaction list as FP32 offsets from the group centre (formed in
+// FP64, then rounded) and are evaluated by all lanes in batches of 32.
 template <bool kTrackSource, int kTPL>
 __global__ void __launch_bounds__(kMixedWarps * 32,
                                    kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : (kTPL == 2 ? NBB_MIXED_MINBLOCKS2 : NBB_MIXED_MINBLOCKS))
@@ -435,119 +439,228 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
     if (lane == 0) stack[0] = root;
     int sp = (m > 0 && root >= 0 && root < m) ? 1 : 0;
     __syncwarp();
-    while (sp > 0) {
-      int k = sp < 32 ? sp : 32;
+    // this warp's stack extension in global memory: when the shared part
+    // fills, its bottom half moves there (the combined stack keeps its
+    // order) and comes back when the shared part runs low
+    int *ext = nullptr;
+    int esp = 0;
+    {
+      const int gw = blockIdx.x * kMixedWarps + wid;
+      if (ws.walk_ext && gw < ws.walk_warps) ext = ws.walk_ext + (size_t)gw * ws.walk_ext_cap;
+    }
+    while (sp > 0 || esp > 0) {
+      if (sp > kStackCap - 7 * kWalkPop && ext && esp + kSpill <= ws.walk_ext_cap) {
+        for (int i = lane; i < kSpill; i += 32) ext[esp + i] = stack[i];
+        __syncwarp();
+        // the destination ends below kSpill, where the sources start
+        for (int i = lane; i < sp - kSpill; i += 32) stack[i] = stack[kSpill + i];
+        esp += kSpill;
+        sp -= kSpill;
+        __syncwarp();
+      } else if (sp < kWalkPop && esp > 0) {
+        const int r = min(esp, kSpill);
+        const int v0 = (lane < sp) ? stack[lane] : 0, v1 = (lane + 32 < sp) ? stack[lane + 32] : 0;
+        __syncwarp();
+        if (lane < sp) stack[r + lane] = v0;
+        if (lane + 32 < sp) stack[r + lane + 32] = v1;
+        for (int i = lane; i < r; i += 32) stack[i] = ext[esp - r + i];
+        sp += r;
+        esp -= r;
+        __syncwarp();
+      }
+      // up to 64 nodes per round, two per lane, fetched in one round trip
+      int k = sp < kWalkPop ? sp : kWalkPop;
       const int room = (kStackCap - sp) / 7;
       if (k > room) k = room > 0 ? room : 1;
-      const int node = (lane < k) ? stack[sp - k + lane] : -1;
+      const int n0 = (lane < k) ? stack[sp - k + lane] : -1;
+      const int n1 = (lane + 32 < k) ? stack[sp - k + 32 + lane] : -1;
       sp -= k;
       __syncwarp();
-      int cat = 0;  // 0 nothing, 1 accepted cell, 2 leaf, 3 open
-      int4 meta = make_int4(0, 0, 0, 0), kid0 = make_int4(-1, -1, -1, -1), kid1 = kid0;
-      double4 a = make_double4(0.0, 0.0, 0.0, 0.0), b = a;
-      double crit = 0.0;
-      if (node >= 0) {
-        // one round trip: record, geometry, radius and children together
-        meta = ws.node_meta[node];
-        a = ws.node_a[node];
-        b = ws.node_b[node];
-        crit = ws.node_c[node].x;
-        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)node * 8);
-        kid0 = kids[0];
-        kid1 = kids[1];
-        if (meta.z > 0) {
-          cat = 2;
-        } else if (a.w != 0.0) {
-          const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
-          bool overlap = true;
-          double d2 = 0.0;
+      int4 m0 = make_int4(0, 0, 0, 0), m1 = m0;
+      int4 k00 = make_int4(-1, -1, -1, -1), k01 = k00, k10 = k00, k11 = k00;
+      double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
+      double cr0 = 0.0, cr1 = 0.0;
+      if (n0 >= 0) {
+        m0 = ws.node_meta[n0];
+        a0 = ws.node_a[n0];
+        b0 = ws.node_b[n0];
+        cr0 = ws.node_c[n0].x;
+        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
+        k00 = kids[0];
+        k01 = kids[1];
+      }
+      if (n1 >= 0) {
+        m1 = ws.node_meta[n1];
+        a1 = ws.node_a[n1];
+        b1 = ws.node_b[n1];
+        cr1 = ws.node_c[n1].x;
+        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
+        k10 = kids[0];
+        k11 = kids[1];
+      }
+      // 0 nothing, 1 accepted cell, 2 leaf, 3 open; the cell's list entry
+      // (centre of mass offset from the group centre, mass) in FP32
+      int cat0 = 0, cat1 = 0;
+      float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
+      {
+        const double4 a = a0, b = b0;
+        if (n0 >= 0) {
+          if (m0.z > 0) {
+            cat0 = 2;
+          } else if (a.w != 0.0) {
+            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
+            bool overlap = true;
+            double d2 = 0.0;
 #pragma unroll
-          for (int ax = 0; ax < 3; ++ax) {
-            const double l = gbox[ax], h = gbox[3 + ax];
-            overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
-            const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
-            d2 = fma(e, e, d2);
+            for (int ax = 0; ax < 3; ++ax) {
+              const double l = gbox[ax], h = gbox[3 + ax];
+              overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
+              const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
+              d2 = fma(e, e, d2);
+            }
+            ++tests;
+            cat0 = (!overlap && d2 > cr0 * cr0) ? 1 : 3;
+            e0 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
           }
-          ++tests;
-          cat = (!overlap && d2 > crit * crit) ? 1 : 3;
         }
       }
-      // opened nodes push their children; a push that would not fit the
-      // stack accepts the node instead (bounded walk, counted)
-      // (a node has at most 8 children: four bits per count)
-      int nch = (cat == 3) ? min(max(meta.w, 0), 8) : 0;
+      {
+        const double4 a = a1, b = b1;
+        if (n1 >= 0) {
+          if (m1.z > 0) {
+            cat1 = 2;
+          } else if (a.w != 0.0) {
+            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
+            bool overlap = true;
+            double d2 = 0.0;
+#pragma unroll
+            for (int ax = 0; ax < 3; ++ax) {
+              const double l = gbox[ax], h = gbox[3 + ax];
+              overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
+              const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
+              d2 = fma(e, e, d2);
+            }
+            ++tests;
+            cat1 = (!overlap && d2 > cr1 * cr1) ? 1 : 3;
+            e1 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
+          }
+        }
+      }
+      // opened nodes push their children (node 0's, then node 1's); a push
+      // that would end past the stack accepts the node instead
+      int nc0 = (cat0 == 3) ? min(max(m0.w, 0), 8) : 0;
+      int nc1 = (cat1 == 3) ? min(max(m1.w, 0), 8) : 0;
       int all_children;
-      const int excl = warp_prefix_small<4>(nch, lt, all_children);
+      const int excl = warp_prefix_small<5>(nc0 + nc1, lt, all_children);
       int pushed = all_children;
       if (sp + all_children > kStackCap) {
-        // the lanes whose children would end past the stack's end accept
-        // their node instead; the pushes before them stand
-        if (nch > 0 && sp + excl + nch > kStackCap) {
-          cat = 1;
-          nch = 0;
+        if (nc0 > 0 && sp + excl + nc0 > kStackCap) {
+          cat0 = 1;
+          nc0 = 0;
           ++overflow;
         }
-        pushed = __reduce_max_sync(kFull, nch > 0 ? excl + nch : 0);
+        if (nc1 > 0 && sp + excl + nc0 + nc1 > kStackCap) {
+          cat1 = 1;
+          nc1 = 0;
+          ++overflow;
+        }
+        pushed = __reduce_max_sync(kFull, (nc0 + nc1 > 0) ? excl + nc0 + nc1 : 0);
       }
-      if (nch > 0) {
-        // children always follow their parent in preorder; anything else is
-        // dropped so the walk stays finite
-        const int kid[8] = {kid0.x, kid0.y, kid0.z, kid0.w, kid1.x, kid1.y, kid1.z, kid1.w};
+      {
+        const int kid[8] = {k00.x, k00.y, k00.z, k00.w, k01.x, k01.y, k01.z, k01.w};
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          if (j < nch) stack[sp + excl + j] = (kid[j] > node && kid[j] < m) ? kid[j] : -1;
+          if (j < nc0) stack[sp + excl + j] = (kid[j] > n0 && kid[j] < m) ? kid[j] : -1;
+      }
+      {
+        const int kid[8] = {k10.x, k10.y, k10.z, k10.w, k11.x, k11.y, k11.z, k11.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          if (j < nc1) stack[sp + excl + nc0 + j] = (kid[j] > n1 && kid[j] < m) ? kid[j] : -1;
       }
       sp += pushed;
-      // accepted cells -> interaction list
-      const unsigned cm = __ballot_sync(kFull, cat == 1);
-      if (cat == 1) {
-        const int pos = ls + __popc(cm & lt);
-        list.put(pos, (float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
+      // accepted cells -> interaction list (fewer than 32 entries before,
+      // at most 64 more)
+      const unsigned cm0 = __ballot_sync(kFull, cat0 == 1);
+      const unsigned cm1 = __ballot_sync(kFull, cat1 == 1);
+      if (cat0 == 1) {
+        const int pos = ls + __popc(cm0 & lt);
+        list.put(pos, e0.x, e0.y, e0.z, e0.w);
         if (kTrackSource) src[pos] = -1;
       }
-      ls += __popc(cm);
+      if (cat1 == 1) {
+        const int pos = ls + __popc(cm0) + __popc(cm1 & lt);
+        list.put(pos, e1.x, e1.y, e1.z, e1.w);
+        if (kTrackSource) src[pos] = -1;
+      }
+      ls += __popc(cm0) + __popc(cm1);
       // reached leaves -> their particles: all at once when they fit
-      const int lc = (cat == 2) ? meta.z : 0;
-      int linc, ltotal;
-      if (__all_sync(kFull, lc < 16)) {
-        linc = warp_prefix_small<4>(lc, lt, ltotal) + lc;
+      const int lc0 = (cat0 == 2) ? m0.z : 0;
+      const int lc1 = (cat1 == 2) ? m1.z : 0;
+      int lexcl, ltotal;
+      if (__all_sync(kFull, lc0 < 16 && lc1 < 16)) {
+        lexcl = warp_prefix_small<5>(lc0 + lc1, lt, ltotal);
       } else {
-        linc = lc;
+        int linc = lc0 + lc1;
         for (int o = 1; o < 32; o <<= 1) {
           const int v = __shfl_up_sync(kFull, linc, o);
           if (lane >= o) linc += v;
         }
         ltotal = __shfl_sync(kFull, linc, 31);
+        lexcl = linc - lc0 - lc1;
       }
       if (ls + ltotal <= kListCap) {
-        for (int j = 0; j < lc; ++j) {
-          const double4 q = ws.pm4[meta.y + j];
-          const int pos = ls + linc - lc + j;
-          list.put(pos, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]), (float)q.w);
-          if (kTrackSource) src[pos] = meta.y + j;
+        const int base = ls + lexcl;
+        double4 q0 = make_double4(0.0, 0.0, 0.0, 0.0), q1 = q0;
+        if (lc0 > 0) q0 = ws.pm4[m0.y];
+        if (lc1 > 0) q1 = ws.pm4[m1.y];
+        if (lc0 > 0) {
+          list.put(base, (float)(q0.x - gbox[6]), (float)(q0.y - gbox[7]), (float)(q0.z - gbox[8]), (float)q0.w);
+          if (kTrackSource) src[base] = m0.y;
+        }
+        if (lc1 > 0) {
+          list.put(base + lc0, (float)(q1.x - gbox[6]), (float)(q1.y - gbox[7]), (float)(q1.z - gbox[8]),
+                   (float)q1.w);
+          if (kTrackSource) src[base + lc0] = m1.y;
+        }
+        for (int j = 1; j < lc0; ++j) {
+          const double4 q = ws.pm4[m0.y + j];
+          list.put(base + j, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]), (float)q.w);
+          if (kTrackSource) src[base + j] = m0.y + j;
+        }
+        for (int j = 1; j < lc1; ++j) {
+          const double4 q = ws.pm4[m1.y + j];
+          list.put(base + lc0 + j, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]),
+                   (float)q.w);
+          if (kTrackSource) src[base + lc0 + j] = m1.y + j;
         }
         ls += ltotal;
         __syncwarp();
         flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
       } else {
+        // rare: the leaves' particles do not fit behind the list; their
+        // ranges stay in registers through the flush
         __syncwarp();
         flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
-        unsigned lm = __ballot_sync(kFull, cat == 2);
-        while (lm) {
-          const int l = __ffs(lm) - 1;
-          lm &= lm - 1;
-          const int first = __shfl_sync(kFull, meta.y, l);
-          const int cnt = __shfl_sync(kFull, meta.z, l);
-          for (int b0 = 0; b0 < cnt; b0 += 32) {
-            const int j = b0 + lane;
-            if (j < cnt) {
-              const double4 q = ws.pm4[first + j];
-              list.put(ls + lane, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]), (float)q.w);
-              if (kTrackSource) src[ls + lane] = first + j;
+        for (int h = 0; h < 2; ++h) {
+          unsigned lm = __ballot_sync(kFull, (h == 0 ? lc0 : lc1) > 0);
+          while (lm) {
+            const int l = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int first = __shfl_sync(kFull, h == 0 ? m0.y : m1.y, l);
+            const int cnt = __shfl_sync(kFull, h == 0 ? lc0 : lc1, l);
+            for (int b0 = 0; b0 < cnt; b0 += 32) {
+              const int j = b0 + lane;
+              if (j < cnt) {
+                const double4 q = ws.pm4[first + j];
+                list.put(ls + lane, (float)(q.x - gbox[6]), (float)(q.y - gbox[7]), (float)(q.z - gbox[8]),
+                         (float)q.w);
+                if (kTrackSource) src[ls + lane] = first + j;
+              }
+              ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
+              __syncwarp();
+              flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
             }
-            ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
-            __syncwarp();
-            flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
           }
         }
       }
@@ -892,6 +1005,15 @@ cudaError_t configure_traversal(Workspace &ws) {
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 2>, kMixedWarps * 32, sms, ws.mixed_grid[1][1]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 4>, kMixedWarps * 32, sms, ws.mixed_grid[0][2]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 4>, kMixedWarps * 32, sms, ws.mixed_grid[1][2]);
+  // The stack extension holds a whole walk: the stack stays sorted by tree
+  // level (a round pops the top and pushes children one level deeper), and
+  // a level's entries are pushed only after every older entry of that level
+  // has been popped, so at most 8 x kWalkPop entries per level are pending.
+  int blocks = 148;
+  for (int t = 0; t < 2; ++t)
+    for (int q = 0; q < 3; ++q) blocks = std::max(blocks, ws.mixed_grid[t][q]);
+  ws.walk_warps = blocks * kMixedWarps;
+  ws.walk_ext_cap = 8 * kWalkPop * (ws.max_level + 1);
   return e;
 }
 

@@ -44,7 +44,7 @@ class StateView(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("n_groups", C.c_int), ("n_octree_nodes", C.c_int), ("interactions", C.c_int64),
-                ("mac_tests", C.c_int64), ("group_size", C.c_int)]
+                ("mac_tests", C.c_int64), ("group_size", C.c_int), ("stack_overflow", C.c_int64)]
 
 
 class TreeExport(C.Structure):

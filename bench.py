@@ -254,7 +254,7 @@ def run_nbb(args, rank, world, local):
         stage_ms, st = sim.profile()
         results[name] = {"ms_per_step": total_ms / args.steps, "step_ms": times, "launches": launches,
                          "stages_ms": stage_ms, "interactions": st.interactions,
-                         "mac_tests": st.mac_tests, "n_groups": st.n_groups,
+                         "mac_tests": st.mac_tests, "stack_overflow": st.stack_overflow, "n_groups": st.n_groups,
                          "n_octree_nodes": st.n_octree_nodes, "group_size": st.group_size}
     # end to end through the public API: pinned host state in, step, state out
     sim = sims["mixed"]
@@ -379,6 +379,8 @@ def bench_nbb(args, rank, world, local):
         "speedup_mixed_vs_fp64": plain["ms_per_step"] / mixed["ms_per_step"],
         "stages_ms": mixed["stages_ms"],
         "interactions": mixed["interactions"], "mac_tests": mixed["mac_tests"],
+        # nodes accepted for lack of stack space (0: the test ran everywhere)
+        "stack_overflow": mixed["stack_overflow"],
         "octree": {"groups": mixed["n_groups"], "nodes": mixed["n_octree_nodes"]},
         "gpu_launches": int(mixed["launches"]),
         "clocks": clocks,

@@ -160,6 +160,9 @@ typedef struct {
   int64_t interactions; /* monopole + leaf-pair interactions evaluated */
   int64_t mac_tests;    /* acceptance tests evaluated */
   int group_size;       /* MIXED: warp target group size in use (32, 64 or 128) */
+  int64_t stack_overflow; /* MIXED: nodes accepted because the walk's stack was
+                             full (their children would not fit); 0 in a walk
+                             that applied the acceptance test everywhere */
 } nbb_stats;
 int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats);
 

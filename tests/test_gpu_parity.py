@@ -456,6 +456,29 @@ def test_mixed_autotuned_group_size(nbb_mod):
         nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, group_size=48))
 
 
+@pytest.mark.parametrize("theta", [0.2, 0.5])
+@pytest.mark.parametrize("group_size", [32, 64, 128])
+def test_mixed_walk_tests_every_node(nbb_mod, theta, group_size):
+    """Plummer N=2^20: the mixed walk never accepts a node for lack of stack
+    space (the shared-memory stack spills to its global extension instead),
+    also at theta = 0.2, whose deep, wide walks fill the shared part."""
+    from nbb import ics
+
+    n = 1 << 20
+    p = ics.plummer(n, seed=0)
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, theta, 0.01, 1.0,
+                                                         precision=nbb_mod.PRECISION_MIXED,
+                                                         group_size=group_size))
+    sim.initialize()
+    st = sim.stats()
+    assert st.stack_overflow == 0
+    rng = np.random.Generator(np.random.Philox(7))
+    tg = np.sort(rng.choice(n, 1024, replace=False)).astype(np.int32)
+    exact = np.stack(nbb_mod.compute_direct_accelerations(p.mass, p.x, p.y, p.z, 1.0, 0.01, targets=tg))
+    a = np.stack(sim.accelerations())[:, tg]
+    assert _rms_rel(a, exact) <= (2e-4 if theta < 0.3 else MIXED_RMS_BOUND)
+
+
 def test_mixed_theta_zero_is_direct(nbb_mod):
     from nbb import ics
 
