@@ -1197,7 +1197,14 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
     const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
     const double crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
     const double c2 = __dmul_rn(crit, crit);
-    ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), 0.0);
+    // the mixed walk's squared acceptance radius for a target box: crit, or
+    // the farthest a point of the cell lies from the centre of mass
+    // (sqrt(3) h + |com - centre|) when that is larger, widened by 2^-40 for
+    // rounding.  A box farther than this from the centre of mass touches no
+    // point of the cell, so no overlap test is needed.
+    const double inner = __fma_rn(1.7320508075688774, h, __dsqrt_rn(o2));
+    const double cm = fmax(crit, inner) * (1.0 + 0x1p-40);
+    ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), cm * cm);
     int j = 0;
     int *kids = ws.node_kids + (size_t)pre * 8;
     for (int o = 7; o >= 0; --o) {

@@ -155,7 +155,7 @@ struct Workspace {
   // traversal layout: depth-first preorder, children visited octant 7 -> 0
   double4 *node_a = nullptr;  // com x, y, z, mass
   double4 *node_b = nullptr;  // centre x, y, z, half size
-  double4 *node_c = nullptr;  // crit, crit^2 lower/upper band, unused
+  double4 *node_c = nullptr;  // crit, crit^2 lower/upper band, mixed walk's squared box radius
   int4 *node_meta = nullptr;  // skip, first particle, particle count, nchild
   int *node_kids = nullptr;   // 8 per node, preorder ids in visit order
   int *walk_ext = nullptr;    // walk_warps x walk_ext_cap: the mixed walk's stack below shared memory

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
 // resident blocks per SM for the two- and four-targets-per-lane instances
 // (more registers per thread for the targets' sums)
 #ifndef NBB_MIXED_MINBLOCKS2
-#define NBB_MIXED_MINBLOCKS2 8
+#define NBB_MIXED_MINBLOCKS2 10
 #endif
 #ifndef NBB_MIXED_MINBLOCKS4
 #define NBB_MIXED_MINBLOCKS4 7
@@ -333,10 +333,12 @@ __device__ __forceinline__ int warp_prefix_small(int v, unsigned lt, int &total)
 // Mixed-precision traversal, one warp per target group of at most 32 x kTPL
 // Morton-consecutive targets inside one parent cell (kTPL targets per lane).
 // The group's bounding box (FP64) replaces the target in the reference's
-// acceptance test: a node is accepted for the whole group when the box does
-// not touch the cell and the box-to-centre-of-mass distance exceeds
-// crit = side/theta + |com - centre|, which implies acceptance for every
-// target in the box.  Nodes are examined 64 at a time (two per lane) from a
+// acceptance test: a node is accepted for the whole group when the
+// box-to-centre-of-mass distance exceeds max(crit, sqrt(3) h + |com -
+// centre|) (crit = side/theta + |com - centre|, h the cell's half side;
+// node_c.w holds the square).  Every target in the box is then farther than
+// crit from the centre of mass and outside the cell, so the reference's test
+// accepts the node for each of them.  Nodes are examined 64 at a time (two per lane) from a
 // warp-private stack in shared memory, each lane fetching both nodes'
 // records and child lists in one round trip; a full stack spills its bottom
 // half to a global extension sized for any walk, so every node gets the
@@ -478,13 +480,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       __syncwarp();
       int4 m0 = make_int4(0, 0, 0, 0), m1 = m0;
       int4 k00 = make_int4(-1, -1, -1, -1), k01 = k00, k10 = k00, k11 = k00;
-      double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0, b0 = a0, b1 = a0;
-      double cr0 = 0.0, cr1 = 0.0;
+      double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
+      double cr0 = 0.0, cr1 = 0.0;  // squared acceptance radius for a target box
       if (n0 >= 0) {
         m0 = ws.node_meta[n0];
         a0 = ws.node_a[n0];
-        b0 = ws.node_b[n0];
-        cr0 = ws.node_c[n0].x;
+        cr0 = ws.node_c[n0].w;
         const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
         k00 = kids[0];
         k01 = kids[1];
@@ -492,8 +493,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       if (n1 >= 0) {
         m1 = ws.node_meta[n1];
         a1 = ws.node_a[n1];
-        b1 = ws.node_b[n1];
-        cr1 = ws.node_c[n1].x;
+        cr1 = ws.node_c[n1].w;
         const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
         k10 = kids[0];
         k11 = kids[1];
@@ -503,45 +503,41 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       int cat0 = 0, cat1 = 0;
       float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
       {
-        const double4 a = a0, b = b0;
+        const double4 a = a0;
         if (n0 >= 0) {
           if (m0.z > 0) {
             cat0 = 2;
           } else if (a.w != 0.0) {
-            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
-            bool overlap = true;
+            // squared distance from the group box to the centre of mass
+            const double com[3] = {a.x, a.y, a.z};
             double d2 = 0.0;
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-              const double l = gbox[ax], h = gbox[3 + ax];
-              overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
-              const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
+              const double e = fmax(0.0, fmax(gbox[ax] - com[ax], com[ax] - gbox[3 + ax]));
               d2 = fma(e, e, d2);
             }
             ++tests;
-            cat0 = (!overlap && d2 > cr0 * cr0) ? 1 : 3;
+            cat0 = (d2 > cr0) ? 1 : 3;
             e0 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
           }
         }
       }
       {
-        const double4 a = a1, b = b1;
+        const double4 a = a1;
         if (n1 >= 0) {
           if (m1.z > 0) {
             cat1 = 2;
           } else if (a.w != 0.0) {
-            const double com[3] = {a.x, a.y, a.z}, cen[3] = {b.x, b.y, b.z};
-            bool overlap = true;
+            // squared distance from the group box to the centre of mass
+            const double com[3] = {a.x, a.y, a.z};
             double d2 = 0.0;
 #pragma unroll
             for (int ax = 0; ax < 3; ++ax) {
-              const double l = gbox[ax], h = gbox[3 + ax];
-              overlap = overlap && h >= cen[ax] - b.w && l <= cen[ax] + b.w;
-              const double e = fmax(0.0, fmax(l - com[ax], com[ax] - h));
+              const double e = fmax(0.0, fmax(gbox[ax] - com[ax], com[ax] - gbox[3 + ax]));
               d2 = fma(e, e, d2);
             }
             ++tests;
-            cat1 = (!overlap && d2 > cr1 * cr1) ? 1 : 3;
+            cat1 = (d2 > cr1) ? 1 : 3;
             e1 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
           }
         }
