@@ -316,17 +316,17 @@ __device__ __forceinline__ void flush_full(const PairList &list, int *src, int &
 
 // Exclusive prefix sum over the warp of a small count v in [0, 2^kBits):
 // one ballot per bit, no chain of dependent shuffles.  `total` receives the
-// warp's sum.
+// warp's sum (one warp reduction instead of a population count per bit: the
+// XU pipe that counts bits also runs the walk's reciprocal square roots).
 template <int kBits>
 __device__ __forceinline__ int warp_prefix_small(int v, unsigned lt, int &total) {
   int excl = 0;
-  total = 0;
 #pragma unroll
   for (int b = 0; b < kBits; ++b) {
     const unsigned m = __ballot_sync(kFull, (v >> b) & 1);
     excl += __popc(m & lt) << b;
-    total += __popc(m) << b;
   }
+  total = __reduce_add_sync(kFull, v);
   return excl;
 }
 
