@@ -1219,13 +1219,23 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
 
 // ------------------------------------------------------ target groups ---
 
-// Target groups for the traversal: every node holding more than group_max
-// particles packs its children with at most group_max particles, in octant
-// (= Morton) order, greedily into runs of at most group_max particles; each
-// run is one group.  Groups are contiguous ranges of the sorted particles,
-// never larger than group_max and never wider than their parent cell, so a
-// warp's targets stay spatially compact (fixed 32-particle slices of the
-// Morton order can straddle the whole system where the curve jumps).
+// Target groups for the traversal.  A subtree is a group candidate when it
+// holds at most group_max particles and is compact: a leaf, a single
+// particle, or a cell at least group_depth levels below its system's root.
+// Every other node splits: a node split only for its count packs its
+// candidate children, in octant (= Morton) order, greedily into runs of at
+// most group_max particles, one group per run; a node split for its size
+// makes each candidate child a group of its own (merging siblings would span
+// the wide cell again).  Groups are contiguous ranges of the sorted
+// particles, never larger than group_max, so a warp's targets stay spatially
+// compact (fixed 32-particle slices of the Morton order can straddle the
+// whole system where the curve jumps; a sparse outer cell holding a few dozen
+// scattered particles gives a box so wide that its walk opens most of the
+// tree).
+__device__ __forceinline__ bool group_compact(const Workspace &ws, int node, int np) {
+  return ws.ocount[node] > 0 || np <= 1 || ws.olevel[node] - ws.sys_levels >= ws.group_depth;
+}
+
 __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
@@ -1233,8 +1243,10 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
     const int gmax = ws.group_max;
     const int np = ws.psub[node];
-    if (np <= gmax) {
-      // a whole system smaller than a group is one group
+    const bool virt = ws.olevel[node] < ws.sys_levels;  // children are other systems
+    const bool compact = !virt && group_compact(ws, node, np);
+    if (!virt && np <= gmax && compact) {
+      // a whole system that is one group
       if (ws.olevel[node] == ws.sys_levels && np > 0) ws.tflag[ws.pfirst[node]] = 1;
       continue;
     }
@@ -1246,18 +1258,19 @@ __global__ void __launch_bounds__(kBlock) group_mark_kernel(Workspace ws) {
         if (f + k >= 0 && f + k < ws.n) ws.tflag[f + k] = 1;
       continue;
     }
-    const bool virt = ws.olevel[node] < ws.sys_levels;  // children are other systems
+    const bool merge = compact;  // split for its count only
     int run = 0;
     for (int o = 0; o < 8; ++o) {
       const int c = ws.children[(size_t)node * 8 + o];
       if (c <= 0 || c >= m) continue;
       const int cp = ws.psub[c];
       if (virt) run = 0;
-      if (cp > gmax) {
+      if (cp > gmax || !group_compact(ws, c, cp)) {
+        // the child splits itself
         run = 0;
         continue;
       }
-      if (run == 0 || run + cp > gmax) {
+      if (!merge || run == 0 || run + cp > gmax) {
         const int f = ws.pfirst[c];
         if (f >= 0 && f < ws.n) ws.tflag[f] = 1;
         run = 0;

@@ -62,6 +62,13 @@ constexpr int kMaxLevels = 16;     // octree levels: 10 spatial + up to 3 above 
 
 // Largest target group supported (two targets per lane of a warp).
 constexpr int kGroupMaxLimit = 128;
+// Shallowest cell depth (below the system's root) whose particles may form
+// one target group; a group spanning a larger cell has a box so wide that its
+// walk opens most of the tree (sparse outskirts).
+#ifndef NBB_GROUP_DEPTH
+#define NBB_GROUP_DEPTH 3
+#endif
+constexpr int kGroupDepth = NBB_GROUP_DEPTH;
 // Largest ensemble: 3 octree levels of system id.
 constexpr int kMaxSystems = 512;
 
@@ -86,6 +93,7 @@ struct Workspace {
   int walk_warps = 0;     // warps of the largest mixed-walk grid
   int walk_ext_cap = 0;   // entries per warp of the mixed walk's stack extension
   int group_max = 32;   // largest octree target group: 32, 64 or 128 (32 x target slots per lane)
+  int group_depth = kGroupDepth;  // shallowest cell (levels below its system's root) a group may span
 
   // key layout: an ensemble's system id sits above the 30 Morton bits and
   // adds sys_levels octree levels above the system roots
