@@ -194,12 +194,11 @@ __global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, Travers
           if (here) resume = meta.x;
         } else {
           const double4 c = ws.node_c[node];
-          const double4 b = ws.node_b[node];
           bool acc = false;
           double ux = 0.0, uy = 0.0, uz = 0.0, uw = 0.0;
           if (here) {
             double dx, dy, dz, d2;
-            acc = accept_fp64(a, b, c, t, dx, dy, dz, d2);
+            acc = accept_fp64(a, ws.node_b + node, c, t, dx, dy, dz, d2);
             if (acc) {
               singular |= !vjp_pair(dx, dy, dz, d2, a.w, g, soft2, cx, cy, cz, ux, uy, uz, uw);
               gtx -= ux;
@@ -392,7 +391,6 @@ __global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, Traversa
         const int4 meta = ws.node_meta[node];
         const double4 a = ws.node_a[node];
         const double4 c = ws.node_c[node];
-        const double4 b = ws.node_b[node];
         if (resume == node) {
           if (meta.z > 0) {
             for (int k = 0; k < meta.z; ++k) {
@@ -408,7 +406,7 @@ __global__ void __launch_bounds__(256) frozen_walk_kernel(Workspace ws, Traversa
             resume = meta.x;
           } else {
             double dx, dy, dz, d2;
-            if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
+            if (accept_fp64(a, ws.node_b + node, c, t, dx, dy, dz, d2)) {
               const double4 aq = node_aq[node];
               const double ex = __dsub_rn(aq.x, tq.x), ey = __dsub_rn(aq.y, tq.y), ez = __dsub_rn(aq.z, tq.z);
               singular |= !point_mass_fp64(ex, ey, ez, sqdist(ex, ey, ez), aq.w, g, soft2, ax, ay, az);

@@ -117,7 +117,6 @@ __global__ void __launch_bounds__(256) potential_tree_kernel(Workspace ws, Trave
         const int4 meta = ws.node_meta[node];
         const double4 a = ws.node_a[node];
         const double4 c = ws.node_c[node];
-        const double4 b = ws.node_b[node];
         if (resume == node) {
           if (meta.z > 0) {
             for (int k = 0; k < meta.z; ++k) {
@@ -134,7 +133,7 @@ __global__ void __launch_bounds__(256) potential_tree_kernel(Workspace ws, Trave
             resume = meta.x;
           } else {
             double dx, dy, dz, d2;
-            if (accept_fp64(a, b, c, t, dx, dy, dz, d2)) {
+            if (accept_fp64(a, ws.node_b + node, c, t, dx, dy, dz, d2)) {
               const double r2 = d2 + soft2;
               if (r2 > 0.0) acc += a.w / sqrt(r2);
               resume = meta.x;

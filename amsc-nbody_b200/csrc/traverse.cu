@@ -77,7 +77,6 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
         const int4 meta = ws.node_meta[node];
         const double4 a = ws.node_a[node];
         const double4 c = ws.node_c[node];
-        const double4 b = ws.node_b[node];
         if (resume == node) {
           if (meta.z > 0) {
             // occupied leaf: exact sum over its particles, self excluded
@@ -96,7 +95,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
             resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
           } else {
             double dx, dy, dz, d2;
-            const bool accept = accept_fp64(a, b, c, t, dx, dy, dz, d2);
+            const bool accept = accept_fp64(a, ws.node_b + node, c, t, dx, dy, dz, d2);
             ++tests;
             if (accept) {
               singular |= !point_mass_fp64(dx, dy, dz, d2, a.w, g, soft2, ax, ay, az);
@@ -413,7 +412,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       }
       __syncwarp();
     }
-    const volatile double *gbox = sh.gbox[wid];
+    const double *gbox = sh.gbox[wid];
     const double gcx = 0.5 * (lo[0] + hi[0]), gcy = 0.5 * (lo[1] + hi[1]),
                  gcz = 0.5 * (lo[2] + hi[2]);
     {

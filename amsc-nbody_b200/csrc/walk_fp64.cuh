@@ -28,11 +28,15 @@ __device__ __forceinline__ double sqdist(double dx, double dy, double dz) {
 }
 
 // barnes_hut.cu:292-322: the acceptance test of target t at a node with
-// records a = (com, mass), b = (centre, half size), c = (crit, crit^2 band).
-// sqrt(d2) > crit is decided on d2 against crit^2 outside a 2^-44 band and by
-// the exact square root inside it; a node containing the target, or at zero
-// distance, is never accepted.  Returns the offset com - t and its square.
-__device__ __forceinline__ bool accept_fp64(const double4 &a, const double4 &b, const double4 &c,
+// records a = (com, mass), c = (crit, crit^2 band, box radius^2) and, at *bp,
+// b = (centre, half size).  sqrt(d2) > crit is decided on d2 against crit^2
+// outside a 2^-44 band and by the exact square root inside it; a node
+// containing the target, or at zero distance, is never accepted.  Beyond the
+// box radius (c.w: (max(crit, sqrt(3) h + |com - centre|) (1 + 2^-40))^2) no
+// point of the cell lies, so the containment test can only fail there and b
+// is read only inside it; the decisions are the reference's in every case.
+// Returns the offset com - t and its square.
+__device__ __forceinline__ bool accept_fp64(const double4 &a, const double4 *bp, const double4 &c,
                                             const double4 &t, double &dx, double &dy, double &dz,
                                             double &d2) {
   dx = __dsub_rn(a.x, t.x);
@@ -40,7 +44,8 @@ __device__ __forceinline__ bool accept_fp64(const double4 &a, const double4 &b, 
   dz = __dsub_rn(a.z, t.z);
   d2 = sqdist(dx, dy, dz);
   bool accept = (d2 > c.z) ? true : (d2 < c.y) ? false : (__dsqrt_rn(d2) > c.x);
-  if (accept) {
+  if (accept && !(d2 > c.w)) {
+    const double4 b = *bp;
     const bool contains = fabs(__dsub_rn(t.x, b.x)) <= b.w && fabs(__dsub_rn(t.y, b.y)) <= b.w &&
                           fabs(__dsub_rn(t.z, b.z)) <= b.w;
     accept = !contains && d2 > 0.0;
