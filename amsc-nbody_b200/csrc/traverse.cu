@@ -80,15 +80,45 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
         if (resume == node) {
           if (meta.z > 0) {
             // occupied leaf: exact sum over its particles, self excluded
-            // (barnes_hut.cu:226-277)
-            for (int k = 0; k < meta.z; ++k) {
+            // (barnes_hut.cu:226-277).  Two particles at a time: their square
+            // roots and divisions are independent and overlap; the sums
+            // still take them in the reference's order.
+            int k = 0;
+            for (; k + 1 < meta.z; k += 2) {
+              const int s0 = meta.y + k, s1 = s0 + 1;
+              const double4 q0 = ws.pm4[s0], q1 = ws.pm4[s1];
+              const double dx0 = __dsub_rn(q0.x, t.x), dy0 = __dsub_rn(q0.y, t.y), dz0 = __dsub_rn(q0.z, t.z);
+              const double dx1 = __dsub_rn(q1.x, t.x), dy1 = __dsub_rn(q1.y, t.y), dz1 = __dsub_rn(q1.z, t.z);
+              double f0, f1;
+              const bool ok0 = point_mass_factor(sqdist(dx0, dy0, dz0), q0.w, g, soft2, f0);
+              const bool ok1 = point_mass_factor(sqdist(dx1, dy1, dz1), q1.w, g, soft2, f1);
+              if (s0 != s && q0.w != 0.0) {
+                singular |= !ok0;
+                if (ok0) {
+                  ax = __fma_rn(f0, dx0, ax);
+                  ay = __fma_rn(f0, dy0, ay);
+                  az = __fma_rn(f0, dz0, az);
+                }
+                ++inter;
+              }
+              if (s1 != s && q1.w != 0.0) {
+                singular |= !ok1;
+                if (ok1) {
+                  ax = __fma_rn(f1, dx1, ax);
+                  ay = __fma_rn(f1, dy1, ay);
+                  az = __fma_rn(f1, dz1, az);
+                }
+                ++inter;
+              }
+            }
+            if (k < meta.z) {
               const int sp = meta.y + k;
-              if (sp == s) continue;
               const double4 q = ws.pm4[sp];
-              if (q.w == 0.0) continue;
-              const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
-              singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
-              ++inter;
+              if (sp != s && q.w != 0.0) {
+                const double dx = __dsub_rn(q.x, t.x), dy = __dsub_rn(q.y, t.y), dz = __dsub_rn(q.z, t.z);
+                singular |= !point_mass_fp64(dx, dy, dz, sqdist(dx, dy, dz), q.w, g, soft2, ax, ay, az);
+                ++inter;
+              }
             }
             resume = meta.x;
           } else if (a.w == 0.0) {

@@ -7,16 +7,23 @@
 
 namespace nbb {
 
-// barnes_hut.cu:76-100: G m (d^2 + eps^2)^-3/2 d, accumulated with the
+// barnes_hut.cu:76-100, the factor G m (d^2 + eps^2)^-3/2 with the
 // reference's operation order.  Returns false on a singular interaction.
+__device__ __forceinline__ bool point_mass_factor(double d2, double m, double g, double soft2, double &f) {
+  const double r2 = __dadd_rn(d2, soft2);
+  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
+  const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
+  f = __dmul_rn(__dmul_rn(g, m), inv3);
+  return !(r2 <= 0.0);
+}
+
+// G m (d^2 + eps^2)^-3/2 d accumulated in the reference's order.  Returns
+// false (and adds nothing) on a singular interaction.
 __device__ __forceinline__ bool point_mass_fp64(double dx, double dy, double dz, double d2,
                                                 double m, double g, double soft2, double &ax,
                                                 double &ay, double &az) {
-  const double r2 = __dadd_rn(d2, soft2);
-  if (r2 <= 0.0) return false;
-  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
-  const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
-  const double f = __dmul_rn(__dmul_rn(g, m), inv3);
+  double f;
+  if (!point_mass_factor(d2, m, g, soft2, f)) return false;
   ax = __fma_rn(f, dx, ax);
   ay = __fma_rn(f, dy, ay);
   az = __fma_rn(f, dz, az);
