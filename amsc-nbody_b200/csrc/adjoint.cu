@@ -174,7 +174,40 @@ __global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, Travers
         const double4 a = ws.node_a[node];
         const bool here = resume == node;
         if (meta.z > 0) {
-          for (int k = 0; k < meta.z; ++k) {
+          // two particles at a time: both products are formed (independent
+          // square roots and divisions) before they are added and scattered
+          // in particle order
+          int k = 0;
+          for (; k + 1 < meta.z; k += 2) {
+            const int s0 = meta.y + k, s1 = s0 + 1;
+            const double4 q0 = ws.pm4[s0], q1 = ws.pm4[s1];
+            const bool act0 = here && s0 != s && q0.w != 0.0;
+            const bool act1 = here && s1 != s && q1.w != 0.0;
+            double u0x = 0.0, u0y = 0.0, u0z = 0.0, u0w = 0.0, u1x = 0.0, u1y = 0.0, u1z = 0.0, u1w = 0.0;
+            if (act0) {
+              const double dx = __dsub_rn(q0.x, t.x), dy = __dsub_rn(q0.y, t.y), dz = __dsub_rn(q0.z, t.z);
+              singular |= !vjp_pair(dx, dy, dz, sqdist(dx, dy, dz), q0.w, g, soft2, cx, cy, cz, u0x, u0y, u0z, u0w);
+            }
+            if (act1) {
+              const double dx = __dsub_rn(q1.x, t.x), dy = __dsub_rn(q1.y, t.y), dz = __dsub_rn(q1.z, t.z);
+              singular |= !vjp_pair(dx, dy, dz, sqdist(dx, dy, dz), q1.w, g, soft2, cx, cy, cz, u1x, u1y, u1z, u1w);
+            }
+            if (act0) {
+              gtx -= u0x;
+              gty -= u0y;
+              gtz -= u0z;
+            }
+            const unsigned who0 = __ballot_sync(kFull, act0);
+            if (who0) scatter4(ab.part_g + s0, who0, lane, u0x, u0y, u0z, u0w);
+            if (act1) {
+              gtx -= u1x;
+              gty -= u1y;
+              gtz -= u1z;
+            }
+            const unsigned who1 = __ballot_sync(kFull, act1);
+            if (who1) scatter4(ab.part_g + s1, who1, lane, u1x, u1y, u1z, u1w);
+          }
+          if (k < meta.z) {
             const int sp = meta.y + k;
             const double4 q = ws.pm4[sp];
             const bool act = here && sp != s && q.w != 0.0;
