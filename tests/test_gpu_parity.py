@@ -441,6 +441,29 @@ def test_mixed_group_sizes(nbb_mod, group_size):
     assert _rms_rel(a, exact) <= MIXED_RMS_BOUND
 
 
+@pytest.mark.parametrize("group_size", [32, 64, 128])
+def test_mixed_group_sizes_on_a_disk(nbb_mod, group_size):
+    """A thin disk with a sparse halo, every group size pinned: target groups
+    stay compact (sparse outer cells split instead of forming one wide group),
+    and the mixed error stays at the plain form's Barnes-Hut level."""
+    from nbb import ics
+
+    n = 65536
+    p = ics.disk_bulge(n, seed=1)
+    rng = np.random.Generator(np.random.Philox(98))
+    tg = np.sort(rng.choice(n, 2048, replace=False)).astype(np.int32)
+    exact = np.stack(nbb_mod.compute_direct_accelerations(p.mass, p.x, p.y, p.z, 1.0, 0.005, targets=tg))
+    plain = np.stack(nbb_mod.compute_accelerations(p, 0.5, 0.005, 1.0))[:, tg]
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.005, 1.0,
+                                                         precision=nbb_mod.PRECISION_MIXED,
+                                                         group_size=group_size))
+    sim.initialize()
+    st = sim.stats()
+    assert st.group_size == group_size and st.stack_overflow == 0
+    a = np.stack(sim.accelerations())[:, tg]
+    assert _rms_rel(a, exact) <= _rms_rel(plain, exact) * 1.05
+
+
 def test_mixed_autotuned_group_size(nbb_mod):
     from nbb import ics
 
