@@ -1033,12 +1033,14 @@ cudaError_t configure_traversal(Workspace &ws) {
   // The stack extension holds a whole walk: the stack stays sorted by tree
   // level (a round pops the top and pushes children one level deeper), and
   // a level's entries are pushed only after every older entry of that level
-  // has been popped, so at most 8 x kWalkPop entries per level are pending.
+  // has been popped, so at most 8 x kWalkPop entries per level are pending;
+  // and a walk pushes each node at most once, so never more than the tree's
+  // node capacity either (small systems take a small extension).
   int blocks = 148;
   for (int t = 0; t < 2; ++t)
     for (int q = 0; q < 3; ++q) blocks = std::max(blocks, ws.mixed_grid[t][q]);
   ws.walk_warps = blocks * kMixedWarps;
-  ws.walk_ext_cap = 8 * kWalkPop * (ws.max_level + 1);
+  ws.walk_ext_cap = std::min(8 * kWalkPop * (ws.max_level + 1), std::max(ws.cap_nodes, 1));
   return e;
 }
 
