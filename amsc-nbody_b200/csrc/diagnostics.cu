@@ -119,14 +119,28 @@ __global__ void __launch_bounds__(256) potential_tree_kernel(Workspace ws, Trave
         const double4 c = ws.node_c[node];
         if (resume == node) {
           if (meta.z > 0) {
-            for (int k = 0; k < meta.z; ++k) {
+            // two particles at a time (independent square roots and
+            // divisions), added in order
+            int k = 0;
+            for (; k + 1 < meta.z; k += 2) {
+              const int s0 = meta.y + k, s1 = s0 + 1;
+              const double4 q0 = ws.pm4[s0], q1 = ws.pm4[s1];
+              const double dx0 = q0.x - t.x, dy0 = q0.y - t.y, dz0 = q0.z - t.z;
+              const double dx1 = q1.x - t.x, dy1 = q1.y - t.y, dz1 = q1.z - t.z;
+              const double r20 = dx0 * dx0 + dy0 * dy0 + dz0 * dz0 + soft2;
+              const double r21 = dx1 * dx1 + dy1 * dy1 + dz1 * dz1 + soft2;
+              const double e0 = q0.w / sqrt(r20), e1 = q1.w / sqrt(r21);
+              if (s0 != s && q0.w != 0.0 && r20 > 0.0) acc += e0;
+              if (s1 != s && q1.w != 0.0 && r21 > 0.0) acc += e1;
+            }
+            if (k < meta.z) {
               const int sp = meta.y + k;
-              if (sp == s) continue;
               const double4 q = ws.pm4[sp];
-              if (q.w == 0.0) continue;
-              const double dx = q.x - t.x, dy = q.y - t.y, dz = q.z - t.z;
-              const double r2 = dx * dx + dy * dy + dz * dz + soft2;
-              if (r2 > 0.0) acc += q.w / sqrt(r2);
+              if (sp != s && q.w != 0.0) {
+                const double dx = q.x - t.x, dy = q.y - t.y, dz = q.z - t.z;
+                const double r2 = dx * dx + dy * dy + dz * dz + soft2;
+                if (r2 > 0.0) acc += q.w / sqrt(r2);
+              }
             }
             resume = meta.x;
           } else if (a.w == 0.0) {
