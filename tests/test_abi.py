@@ -65,3 +65,35 @@ def test_library_fails_loudly_without_device():
 
     with pytest.raises((nbb.NoDevice, nbb.DeviceError)):
         nbb.compute_accelerations((np.ones(4), np.arange(4.0), np.zeros(4), np.zeros(4)), 0.5, 0.01)
+
+
+# The ctypes mirrors in nbb/_lib.py and the C structs they stand for.
+STRUCTS = {"Config": "nbb_config", "StateView": "nbb_state_view", "Stats": "nbb_stats",
+           "TreeExport": "nbb_tree_export", "Diagnostics": "nbb_diagnostics", "OctreeView": "nbb_octree_view"}
+
+
+def test_python_structs_match_the_header_layout(tmp_path):
+    """Every struct the Python binding passes through the C ABI has the size
+    and field offsets the compiler gives the header's declaration."""
+    import nbb._lib as L
+
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "nbb.h"', 'int main(void) {']
+    for py, c in STRUCTS.items():
+        lines.append(f'  printf("{py} sizeof %zu\\n", sizeof({c}));')
+        for field, _ in getattr(L, py)._fields_:
+            lines.append(f'  printf("{py} {field} %zu\\n", offsetof({c}, {field}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    exe = tmp_path / "layout"
+    src.write_text("\n".join(lines) + "\n")
+    subprocess.check_call(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                           str(src), "-o", str(exe)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        py, field, value = line.split()
+        got[(py, field)] = int(value)
+    for py in STRUCTS:
+        cls = getattr(L, py)
+        assert got[(py, "sizeof")] == ctypes.sizeof(cls), py
+        for field, _ in cls._fields_:
+            assert got[(py, field)] == getattr(cls, field).offset, (py, field)
