@@ -235,12 +235,21 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 // same FP64 difference -- and contributes exactly zero, so no source index is
 // needed.  With zero softening the source index excludes self and detects
 // the reference's singular interaction (returns true).
+// Pairs per unrolled block of the evaluation loop, by the walk's target
+// slots per lane (its register budget): 8 for one or two slots, 4 for four
+// (8 spills there).
 #ifndef NBB_EVAL_UNROLL
-#define NBB_EVAL_UNROLL 4
+#define NBB_EVAL_UNROLL 8
 #endif
-constexpr int kEvalUnroll = NBB_EVAL_UNROLL;  // pairs per unrolled block of the evaluation loop
+#ifndef NBB_EVAL_UNROLL4
+#define NBB_EVAL_UNROLL4 4
+#endif
+template <int kSlots>
+__host__ __device__ constexpr int eval_unroll() {
+  return kSlots >= 4 ? NBB_EVAL_UNROLL4 : NBB_EVAL_UNROLL;
+}
 
-template <bool kTrackSource, int kTPL>
+template <bool kTrackSource, int kTPL, int kUnroll>
 __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src, int count, const int *self,
                                            const float2 *ntx, const float2 *nty, const float2 *ntz, float2 eps2,
                                            float3 *sum, float3 *comp) {
@@ -250,7 +259,7 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
   const float2 neg_half = make_float2(-0.5f, -0.5f), three_halves = make_float2(1.5f, 1.5f);
   bool singular = false;
   const int pairs = (count + 1) >> 1;
-#pragma unroll kEvalUnroll
+#pragma unroll kUnroll
   for (int pr = 0; pr < pairs; ++pr) {
     const float4 ea = list.a[pr], eb = list.b[pr];
     const float2 ex = make_float2(ea.x, ea.y), ey = make_float2(ea.z, ea.w);
@@ -303,15 +312,15 @@ template <bool kTrackSource, int kTPL>
 __device__ __forceinline__ bool eval_slots(const PairList &list, const int *src, int count, int nq,
                                            LaneTargets<kTPL> &t, float2 eps2) {
   if (kTPL >= 4 && nq >= 4)
-    return eval_batch<kTrackSource, (kTPL >= 4 ? 4 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 4 ? 4 : 1), eval_unroll<kTPL>()>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
   if (kTPL >= 3 && nq == 3)
-    return eval_batch<kTrackSource, (kTPL >= 3 ? 3 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 3 ? 3 : 1), eval_unroll<kTPL>()>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
   if (kTPL >= 2 && nq == 2)
-    return eval_batch<kTrackSource, (kTPL >= 2 ? 2 : 1)>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
+    return eval_batch<kTrackSource, (kTPL >= 2 ? 2 : 1), eval_unroll<kTPL>()>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum,
                                                          t.comp);
-  return eval_batch<kTrackSource, 1>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum, t.comp);
+  return eval_batch<kTrackSource, 1, eval_unroll<kTPL>()>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum, t.comp);
 }
 
 template <bool kTrackSource, int kTPL>
