@@ -1,7 +1,7 @@
 // adjoint.cu -- reverse-mode derivative of the Barnes-Hut force with the tree
 // frozen, a frozen-structure replay for finite differences, and the FP64
 // direct-sum adjoint.  None of this has a counterpart in sytrams/AMSC-Nbody;
-// the force being differentiated is the plain form of barnes_hut.cu:184-342.
+// the force being differentiated is the plain form of barnes_hut.cu:164-322.
 //
 // Force with frozen structure.  For target i with accepted-node set A_i and
 // opened-leaf particle set L_i (both decided by the reference's acceptance

@@ -2,21 +2,21 @@
 //
 // Stage map (reference file:line each kernel replaces, paths relative to the
 // sytrams/AMSC-Nbody project root):
-//   kd_bbox_kernel        integrator.cu:57-89 (KD) fused with
-//                         globalbounding.cu:130-180 (Bbox)
-//   encode_kernel         morton.cu:147-188 (normalise/quantise/interleave)
+//   kd_bbox_kernel        integrator.cu:51-83 (KD) fused with
+//                         globalbounding.cu:94-144 (Bbox)
+//   encode_kernel         morton.cu:98-139,160-219 (normalise/quantise/interleave)
 //                         + the digit histograms of the radix sort
-//   onesweep_kernel       morton.cu:270-273 (stable_sort_by_key), in-house
+//   onesweep_kernel       morton.cu:221-224 (stable_sort_by_key), in-house
 //                         LSD radix sort with decoupled look-back
-//   groups_kernel         morton_leaf_groups.cu:105-150 (RLE + scan) fused
+//   groups_kernel         morton_leaf_groups.cu:58-103 (RLE + scan) fused
 //                         with simulation.cu:34-58 (Morton-order gather)
 //   karras_kernel         tree_builder.cu:9-113
-//   plan_kernel           radix_to_octree.cu:140-215 + its exclusive scan
-//   octree_clear_kernel   octree_builder.cu:476-509 (initialisation)
-//   materialize_kernel    octree_builder.cu:275-412
-//   node_init_kernel      octree_geometry.cu:56-102 + octree_physics.cu:236-326
+//   plan_kernel           radix_to_octree.cu:70-145 + its exclusive scan
+//   octree_clear_kernel   octree_builder.cu:288-321 (initialisation)
+//   materialize_kernel    octree_builder.cu:87-224
+//   node_init_kernel      octree_geometry.cu:56-102 + octree_physics.cu:64-154
 //   level_bin_kernel      octree nodes binned by level
-//   propagate_level_kernel octree_physics.cu:328-417 (+ subtree sizes), one
+//   propagate_level_kernel octree_physics.cu:156-245 (+ subtree sizes), one
 //                         level per launch, deepest first
 //   pre_level_kernel      preorder indices, one level per launch, root first
 //   layout_kernel         traversal records in depth-first preorder
@@ -91,7 +91,7 @@ __device__ __forceinline__ T warp_reduce_max(T v) {
   return v;
 }
 
-// Box of one system from its encoded extrema (globalbounding.cu:158-172):
+// Box of one system from its encoded extrema (globalbounding.cu:122-136):
 // centre = (min + max) * 0.5, side = 1.1 * longest extent, 1 when that is 0.
 __device__ void finish_box(const unsigned long long *mn, const unsigned long long *mx, double *box) {
   double lo[3], hi[3];
@@ -111,8 +111,8 @@ __device__ void finish_box(const unsigned long long *mn, const unsigned long lon
 }
 
 // One pass over the state: optional first half kick + drift
-// (integrator.cu:57-89), then the extrema of the new positions and a
-// non-finite flag (globalbounding.cu:62-92), per system.  The last block to
+// (integrator.cu:51-83), then the extrema of the new positions and a
+// non-finite flag (globalbounding.cu:17-56), per system.  The last block to
 // finish forms every system's box.  A single system reduces through shared
 // memory with one set of atomics per block; an ensemble (systems stored
 // contiguously) reduces per warp when the warp's particles share a system
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kBlock) kd_bbox_kernel(Workspace ws, double dt
 
 // ---------------------------------------------------- Morton encode ----
 
-// morton.cu:168-177
+// morton.cu:119-128
 __device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
   uint32_t x = v & 0x000003FFu;
   x = (x | (x << 16)) & 0x030000FFu;
@@ -241,7 +241,7 @@ __device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
   return x;
 }
 
-// morton.cu:147-166 with explicitly rounded operations: the normalised
+// morton.cu:98-117 with explicitly rounded operations: the normalised
 // coordinate is a true division, then scaled by the 1024-cell grid, clamped
 // to [0, 1023] and truncated.
 __device__ __forceinline__ uint32_t quantise(double a, double lower, double side) {
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(kBlock) encode_kernel(Workspace ws) {
   const int n = ws.n;
   const bool multi = ws.n_systems > 1;
   if (blockIdx.x == 0) {
-    // morton.cu:218-219, every system's box
+    // morton.cu:167-170, every system's box
     for (int sys = threadIdx.x; sys < ws.n_systems; sys += blockDim.x) {
       const double *b = ws.sys_box + 4 * (size_t)sys;
       if (!isfinite(b[0]) || !isfinite(b[1]) || !isfinite(b[2]) || !isfinite(b[3]) || b[3] <= 0.0)
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(kBlock)
 
 // -------------------------------------------------------------- plan ----
 
-// radix_to_octree.cu:124-138.  Spatial prefix bits = prefix length in the
+// radix_to_octree.cu:54-68.  Spatial prefix bits = prefix length in the
 // reference's 32-bit frame minus (32 - key bits); for a single system (30-bit
 // keys) that is the reference's plen - 2.
 __device__ __forceinline__ int octree_level_of(const Workspace &ws, int n_leaves, int r) {
@@ -679,7 +679,7 @@ __device__ __forceinline__ int octree_level_of(const Workspace &ws, int n_leaves
   return prefix / kDims;
 }
 
-// radix_to_octree.cu:140-215 for radix node r; returns the edge node count.
+// radix_to_octree.cu:70-145 for radix node r; returns the edge node count.
 __device__ int plan_node(const Workspace &ws, int g, int r) {
   const int nr = 2 * g - 1;
   DevScalars *sc = ws.sc;
@@ -710,7 +710,7 @@ __device__ int plan_node(const Workspace &ws, int g, int r) {
 }
 
 // Plan values + their exclusive scan in one pass; the last tile sets
-// M = 1 + sum (radix_to_octree.cu:291-313), bounded by the node capacity.
+// M = 1 + sum (radix_to_octree.cu:221-243), bounded by the node capacity.
 __global__ void __launch_bounds__(kScanThreads) plan_kernel(Workspace ws) {
   __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
   __shared__ unsigned long long s_total, s_prefix;
@@ -756,7 +756,7 @@ __global__ void __launch_bounds__(kScanThreads) plan_kernel(Workspace ws) {
 
 // ------------------------------------------------------------ octree ----
 
-// octree_builder.cu:476-509: empty child slots and parents -1, root level 0.
+// octree_builder.cu:288-321: empty child slots and parents -1, root level 0.
 __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
   const int m = ws.sc->n_nodes;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(kBlock) octree_clear_kernel(Workspace ws) {
   }
 }
 
-// octree_builder.cu:237-254 for keys of key_bits bits.
+// octree_builder.cu:49-85 for keys of key_bits bits.
 __device__ __forceinline__ unsigned long long prefix_at_level(unsigned long long key, int level, int key_bits) {
   if (level == 0) return 0ull;
   const int rem = key_bits - level * kDims;
@@ -790,7 +790,7 @@ __device__ __forceinline__ int octant_at_level(unsigned long long key, int level
   return (int)((key >> (key_bits - level * kDims)) & 7ull);
 }
 
-// octree_builder.cu:275-412: each radix edge emits its chain of octree nodes
+// octree_builder.cu:87-224: each radix edge emits its chain of octree nodes
 // at ids 1 + edgeNodeOffset[r] + k; children slots are claimed with
 // atomicCAS so a collision is detected as the reference does.
 __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
@@ -899,9 +899,9 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
 // -------------------------------------------- geometry + leaf physics ----
 
 // Per node: cell centre / half size from the Morton prefix path
-// (octree_geometry.cu:56-102), child count (octree_physics.cu:236-265) and,
+// (octree_geometry.cu:56-102), child count (octree_physics.cu:64-93) and,
 // for occupied leaves, mass and centre of mass summed over the group's
-// particles in sorted order (octree_physics.cu:267-326).
+// particles in sorted order (octree_physics.cu:95-154).
 __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
@@ -1046,7 +1046,7 @@ __global__ void __launch_bounds__(kBlock) level_bin_kernel(Workspace ws) {
   }
 }
 
-// octree_physics.cu:328-417, one octree level per launch, deepest first:
+// octree_physics.cu:156-245, one octree level per launch, deepest first:
 // every internal node of the level combines its (finished) children in
 // octant order 0..7 -- the reference's deterministic order, so mass and
 // centre of mass are bit-identical -- and also sums its subtree size,
@@ -1128,13 +1128,13 @@ __global__ void __launch_bounds__(kBlock) propagate_level_kernel(Workspace ws, i
 // --------------------------------------------------------------- layout --
 
 // Traversal records in depth-first preorder with children visited octant
-// 7 -> 0 (the reference's traversal order, barnes_hut.cu:110-182).  Preorder
+// 7 -> 0 (the reference's traversal order, barnes_hut.cu:90-162).  Preorder
 // indices go top-down, one octree level per launch: node n sits at
 // pre(n) = pre(parent) + its offset within the parent's range; then one
 // launch over all nodes writes the records.  Its
 // subtree ends at pre(n) + size(n) ("skip"), and its children are listed in
 // visit order.  The acceptance radius crit = side/theta + |com - centre|
-// (barnes_hut.cu:297-311) is precomputed once per node, with a +-2^-44 band
+// (barnes_hut.cu:283-293) is precomputed once per node, with a +-2^-44 band
 // around crit^2 inside which the traversal falls back to the exact
 // sqrt(d^2) > crit comparison.
 __global__ void __launch_bounds__(kBlock) pre_level_kernel(Workspace ws, int level) {

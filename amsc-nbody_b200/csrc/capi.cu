@@ -76,7 +76,7 @@ const char *device_message(int stage, int code) {
     case kStageBbox:
       return code == 1 ? "Particle positions must be finite to compute a bounding box."
                        : "Morton bounding box is not valid";
-    case kStagePlan:  // radix_to_octree.cu:102-121
+    case kStagePlan:  // radix_to_octree.cu:32-51
       switch (code) {
         case 1: return "A Morton key uses bits outside the configured 30-bit spatial layout";
         case 2: return "A radix node has an invalid parent";
@@ -85,7 +85,7 @@ const char *device_message(int stage, int code) {
         case kCodeOverflow: return "The computed octree node count exceeds the node capacity";
         default: return "Unknown radix-to-octree planning error";
       }
-    case kStageOctree:  // octree_builder.cu:206-234
+    case kStageOctree:  // octree_builder.cu:18-46
       switch (code) {
         case 1: return "Invalid radix edge metadata";
         case 2: return "Invalid radix ancestor while constructing octree";
@@ -99,7 +99,7 @@ const char *device_message(int stage, int code) {
     case kStageGeometry:  // octree_geometry.cu:21-34
       return code == 1 ? "Octree node has an invalid level"
                        : code == 2 ? "Octree node has an invalid Morton prefix" : "Unknown octree geometry error";
-    case kStagePhysics:  // octree_physics.cu:190-218
+    case kStagePhysics:  // octree_physics.cu:18-46
       switch (code) {
         case 1: return "Octree contains an invalid child ID";
         case 2: return "Occupied octree leaf has invalid particle range";
@@ -110,7 +110,7 @@ const char *device_message(int stage, int code) {
         case 7: return "An octree parent was signalled too many times";
         default: return "Unknown octree physics error";
       }
-    case kStageTraversal:  // barnes_hut.cu:41-72
+    case kStageTraversal:  // barnes_hut.cu:21-52
       switch (code) {
         case 1: return "Barnes-Hut traversal found an invalid child node";
         case 2: return "Barnes-Hut traversal found an invalid leaf particle range";
@@ -472,7 +472,7 @@ int nbb_last_error_code(void) { return t_code; }
 uint64_t nbb_kernel_launch_count(void) { return nbb::launch_count(); }
 
 static int validate_config(const nbb_config *c) {
-  // simulation.cpp:21-33, barnes_hut.cu:376-383
+  // simulation.cpp:21-33, barnes_hut.cu:355-363
   if (!std::isfinite(c->time_step) || c->time_step <= 0.0)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Simulation timeStep must be finite and positive");
   if (!finite_nonneg(c->theta))
@@ -1156,7 +1156,7 @@ int nbb_accel_direct(size_t n, const double *mass, const double *x, const double
 int nbb_accel_octree(const nbb_octree_view *o, const uint32_t *idx, const double *mass, const double *x,
                      const double *y, const double *z, double *ax, double *ay, double *az, double theta,
                      double softening, double g, int particle_order, int on_device) {
-  // barnes_hut.cu:345-391 validation
+  // barnes_hut.cu:325-391 validation
   if (!o || o->n_particles <= 0 || o->n_nodes <= 0)
     return fail(NBB_ERR_LOGIC, "Octree is not valid for Barnes-Hut traversal");
   if (!o->children || !o->parent || !o->first || !o->count)
@@ -1221,7 +1221,7 @@ int nbb_accel_octree(const nbb_octree_view *o, const uint32_t *idx, const double
 
 int nbb_kick_drift(double *x, double *y, double *z, double *vx, double *vy, double *vz, const double *ax,
                    const double *ay, const double *az, size_t n, double dt, void *stream) {
-  // integrator.cu:115-132
+  // integrator.cu:109-126
   if (!std::isfinite(dt) || dt <= 0.0)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog timestep must be finite and positive");
   if (n == 0) return ok();
@@ -1236,7 +1236,7 @@ int nbb_kick_drift(double *x, double *y, double *z, double *vx, double *vy, doub
 
 int nbb_kick(double *vx, double *vy, double *vz, const double *ax, const double *ay, const double *az, size_t n,
              double dt, void *stream) {
-  // integrator.cu:135-151
+  // integrator.cu:129-145
   if (!std::isfinite(dt) || dt <= 0.0)
     return fail(NBB_ERR_INVALID_ARGUMENT, "Leapfrog timestep must be finite and positive");
   if (n == 0) return ok();

@@ -22,11 +22,11 @@ enum Stage : int {
   kStageBbox = 1,       // code 1 non-finite position, 2 invalid box
   kStageSort = 2,       // code 99 bounded look-back wait gave up
   kStageGroups = 3,     // code 99 bounded look-back wait gave up
-  kStagePlan = 4,       // radix_to_octree.cu:102-121 codes 1..4; 90 overflow
-  kStageOctree = 5,     // octree_builder.cu:206-234 codes 1..7
+  kStagePlan = 4,       // radix_to_octree.cu:32-51 codes 1..4; 90 overflow
+  kStageOctree = 5,     // octree_builder.cu:18-46 codes 1..7
   kStageGeometry = 6,   // octree_geometry.cu:21-34 codes 1..2
-  kStagePhysics = 7,    // octree_physics.cu:190-218 codes 1..7
-  kStageTraversal = 8,  // barnes_hut.cu:41-72 codes 1..8
+  kStagePhysics = 7,    // octree_physics.cu:18-46 codes 1..7
+  kStageTraversal = 8,  // barnes_hut.cu:21-52 codes 1..8
   kStageLayout = 9      // code 1 inconsistent preorder walk
 };
 constexpr int kCodeTimeout = 99;

@@ -1,6 +1,6 @@
 // traverse.cu -- Barnes-Hut force evaluation on sm_100a.
 //
-//  traverse_fp64_kernel   plain form of barnes_hut.cu:184-342 (paths relative
+//  traverse_fp64_kernel   plain form of barnes_hut.cu:164-322 (paths relative
 //                         to the sytrams/AMSC-Nbody project root): per-target
 //                         acceptance test and interaction order identical to
 //                         the reference, FP64 throughout.
@@ -9,7 +9,7 @@
 //  direct_kernel          FP64 direct summation (theta-error oracle).
 //  ref_octree_kernel      traversal of a caller octree in the reference's own
 //                         node numbering (function-level API).
-//  kick / kick_drift      integrator.cu:57-112.
+//  kick / kick_drift      integrator.cu:51-106.
 #include "nbb_internal.cuh"
 #include "walk_fp64.cuh"
 
@@ -31,7 +31,7 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
 // Plain FP64 traversal, one warp per 32 Morton-consecutive targets.
 //
 // The tree is laid out in depth-first preorder with children visited octant
-// 7 -> 0, so the reference's per-thread stackless walk (barnes_hut.cu:110-182)
+// 7 -> 0, so the reference's per-thread stackless walk (barnes_hut.cu:90-162)
 // becomes: a target opened at node i continues at i + 1, a target done with
 // node i (accepted, zero mass, or a leaf) continues at skip(i).  Each lane
 // keeps its own resume index and the warp always visits the smallest one, so
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
         if (resume == node) {
           if (meta.z > 0) {
             // occupied leaf: exact sum over its particles, self excluded
-            // (barnes_hut.cu:226-277).  Two particles at a time: their square
+            // (barnes_hut.cu:204-257).  Two particles at a time: their square
             // roots and divisions are independent and overlap; the sums
             // still take them in the reference's order.
             int k = 0;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
             }
             resume = meta.x;
           } else if (a.w == 0.0) {
-            resume = meta.x;  // zero-mass node (barnes_hut.cu:282-291)
+            resume = meta.x;  // zero-mass node (barnes_hut.cu:259-271)
           } else {
             double dx, dy, dz, d2;
             const bool accept = accept_fp64(a, ws.node_b + node, c, t, dx, dy, dz, d2);
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) traverse_fp64_kernel(Workspace ws, Traver
         ws.ay[ti] = ay;
         ws.az[ti] = az;
         if (p.kick) {
-          // second half kick, integrator.cu:92-112
+          // second half kick, integrator.cu:86-106
           ws.vx[ti] = __fma_rn(p.half_dt, ax, ws.vx[ti]);
           ws.vy[ti] = __fma_rn(p.half_dt, ay, ws.vy[ti]);
           ws.vz[ti] = __fma_rn(p.half_dt, az, ws.vz[ti]);
@@ -796,7 +796,7 @@ __global__ void __launch_bounds__(kDirectThreads)
 
 // ------------------------------------------- reference-layout octree ----
 
-// barnes_hut.cu:110-182 on a caller octree in the reference numbering.
+// barnes_hut.cu:90-162 on a caller octree in the reference numbering.
 __device__ int ref_first_child(const RefOctree &o, int node, int &err) {
   for (int oc = 7; oc >= 0; --oc) {
     const int c = o.children[node * 8 + oc];

@@ -7,7 +7,7 @@
 
 namespace nbb {
 
-// barnes_hut.cu:76-100, the factor G m (d^2 + eps^2)^-3/2 with the
+// barnes_hut.cu:56-80, the factor G m (d^2 + eps^2)^-3/2 with the
 // reference's operation order.  Returns false on a singular interaction.
 __device__ __forceinline__ bool point_mass_factor(double d2, double m, double g, double soft2, double &f) {
   const double r2 = __dadd_rn(d2, soft2);
@@ -34,7 +34,7 @@ __device__ __forceinline__ double sqdist(double dx, double dy, double dz) {
   return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
 }
 
-// barnes_hut.cu:292-322: the acceptance test of target t at a node with
+// barnes_hut.cu:273-294: the acceptance test of target t at a node with
 // records a = (com, mass), c = (crit, crit^2 band, box radius^2) and, at *bp,
 // b = (centre, half size).  sqrt(d2) > crit is decided on d2 against crit^2
 // outside a 2^-44 band and by the exact square root inside it; a node

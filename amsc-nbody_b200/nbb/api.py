@@ -55,7 +55,7 @@ class BarnesHutParameters:
 
 class Simulation:
     """Owns the particle state on the GPU and advances it with leapfrog KDK
-    (src/simulation.cpp:286-343).  ``particles`` is copied in."""
+    (src/simulation.cpp:70-127).  ``particles`` is copied in."""
 
     def __init__(self, particles: ParticleData, config: SimulationConfig, types=None):
         lib = _lib.load()
@@ -284,7 +284,7 @@ def compute_accelerations(particles_or_arrays, theta: float, softening: float, g
                           precision: int = _lib.PRECISION_FP64, export: bool = False,
                           stats: bool = False):  # noqa: D417
     """One rebuild + Barnes-Hut evaluation of caller particles (host arrays):
-    the reference's pipeline of src/simulation.cpp:353-414 with an explicit
+    the reference's pipeline of src/simulation.cpp:137-198 with an explicit
     G.  Returns (ax, ay, az) [, export dict] [, Stats]."""
     lib = _lib.load()
     if isinstance(particles_or_arrays, ParticleData):

@@ -14,7 +14,7 @@
  * code.  A simulation handle that reported an error other than
  * NBB_ERR_INVALID_ARGUMENT / NBB_ERR_LOGIC on a step is unusable afterwards,
  * as the reference's Simulation enters State::failed
- * (src/simulation.cpp:316-335).
+ * (src/simulation.cpp:100-119).
  *
  * Threading: a handle is not thread-safe; distinct handles are independent.
  */
@@ -43,7 +43,7 @@ typedef enum {
 } nbb_status;
 
 /* Traversal arithmetic.  FP64 is the reference's plain form
- * (gpu/cuda_kernels/barnes_hut.cu:184-342): per-target acceptance test and
+ * (gpu/cuda_kernels/barnes_hut.cu:164-322): per-target acceptance test and
  * interaction sets, FP64 throughout.  MIXED evaluates the interaction bulk in
  * FP32 (offsets formed in FP64 and rounded, rsqrtf + one Newton step,
  * Kahan-compensated partial sums) over interaction lists shared by a warp
@@ -71,7 +71,7 @@ void nbb_config_default(nbb_config *cfg);
 
 typedef struct nbb_sim nbb_sim;
 
-/* Simulation(Particles, SimulationConfig) (src/simulation.cpp:286-290):
+/* Simulation(Particles, SimulationConfig) (src/simulation.cpp:70-74):
  * validates the configuration and copies the planar state in (host pointers
  * when on_device == 0, device pointers otherwise).  type may be NULL. */
 int nbb_sim_create(const nbb_config *cfg, size_t n, const double *mass,
@@ -92,17 +92,17 @@ int nbb_ensemble_create(const nbb_config *cfg, int n_systems,
                         const double *z, const double *vx, const double *vy,
                         const double *vz, int on_device, nbb_sim **out);
 
-/* Simulation::initialize (src/simulation.cpp:294-314): first spatial build
+/* Simulation::initialize (src/simulation.cpp:78-98): first spatial build
  * and acceleration; NBB_ERR_LOGIC when called twice. */
 int nbb_sim_initialize(nbb_sim *sim);
 
-/* Simulation::step / run (src/simulation.cpp:316-343): KD, rebuild, force,
+/* Simulation::step / run (src/simulation.cpp:100-127): KD, rebuild, force,
  * K.  No host synchronisation inside a step; the call synchronises once at
  * its end to report device errors. */
 int nbb_sim_step(nbb_sim *sim);
 int nbb_sim_run(nbb_sim *sim, uint64_t steps);
 
-/* Simulation::time / stepNumber (src/simulation.cpp:345-347) */
+/* Simulation::time / stepNumber (src/simulation.cpp:129-131) */
 double nbb_sim_time(const nbb_sim *sim);
 uint64_t nbb_sim_step_number(const nbb_sim *sim);
 
@@ -202,8 +202,8 @@ int nbb_sim_export(nbb_sim *sim, nbb_tree_export *out);
 /* One spatial build + Barnes-Hut evaluation on caller particles, the
  * sequence Bbox -> MortonKeys -> allocate/build{MortonLeafGroups, Tree,
  * RadixToOctreePlan, Octree, geometry, physics} ->
- * computeBarnesHutAcceleration (src/simulation.cpp:353-414,
- * gpu/cuda_kernels/barnes_hut.cu:345-391).  Accelerations are written at the
+ * computeBarnesHutAcceleration (src/simulation.cpp:137-198,
+ * gpu/cuda_kernels/barnes_hut.cu:325-391).  Accelerations are written at the
  * original particle index.  Pointers are host (on_device == 0) or device.
  * export_out and stats may be NULL. */
 int nbb_accel(size_t n, const double *mass, const double *x, const double *y,
@@ -221,7 +221,7 @@ int nbb_accel_direct(size_t n, const double *mass, const double *x,
                      double *ax, double *ay, double *az, int on_device);
 
 /* computeBarnesHutAcceleration on a caller-built octree
- * (gpu/cuda_kernels/barnes_hut.cu:345-391), FP64 plain form.  Octree arrays
+ * (gpu/cuda_kernels/barnes_hut.cu:325-391), FP64 plain form.  Octree arrays
  * follow src/octree_types.hpp:73-104 (children node-major, 8 per node; root
  * 0).  particle_order: 0 = original, 1 = morton (BarnesHutParticleOrder). */
 typedef struct {
@@ -334,9 +334,9 @@ int nbb_sim_diagnostics(nbb_sim *sim, int potential, nbb_diagnostics *out);
 /* ---------------------------------------------------------------------------
  * Differentiable rollout.  No counterpart in the reference (which has no
  * derivative of its step); the force differentiated is the plain FP64
- * Barnes-Hut force of src/barnes_hut.cu:184-342 with the tree topology and
- * every target's accepted-node and opened-leaf sets held fixed at the
- * positions of each step.
+ * Barnes-Hut force of gpu/cuda_kernels/barnes_hut.cu:164-322 with the tree
+ * topology and every target's accepted-node and opened-leaf sets held fixed
+ * at the positions of each step.
  *
  * nbb_sim_rollout advances an initialized simulation by `steps` steps (as
  * nbb_sim_run) and keeps (x, v, a) every `checkpoint_every` steps on the

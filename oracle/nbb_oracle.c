@@ -39,12 +39,12 @@ static void set_threads(int n_threads) {
 
 int orc_bbox(size_t n, const double *x, const double *y, const double *z,
              double out[4]) {
-  /* globalbounding.cu:132-135: empty input is rejected. */
+  /* globalbounding.cu:96-99: empty input is rejected. */
   if (n == 0) return ORC_EINVAL;
   double lo[3] = {INFINITY, INFINITY, INFINITY};
   double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   int non_finite = 0;
-  /* globalbounding.cu:62-92: per-particle degenerate box, component-wise
+  /* globalbounding.cu:17-56: per-particle degenerate box, component-wise
    * fmin/fmax combine, non-finite flag OR-ed. */
   for (size_t i = 0; i < n; ++i) {
     const double p[3] = {x[i], y[i], z[i]};
@@ -54,9 +54,9 @@ int orc_bbox(size_t n, const double *x, const double *y, const double *z,
       hi[a] = fmax(hi[a], p[a]);
     }
   }
-  /* globalbounding.cu:153-156 */
+  /* globalbounding.cu:117-120 */
   if (non_finite) return ORC_EDOMAIN;
-  /* globalbounding.cu:158-172 */
+  /* globalbounding.cu:122-136 */
   out[0] = (lo[0] + hi[0]) * 0.5;
   out[1] = (lo[1] + hi[1]) * 0.5;
   out[2] = (lo[2] + hi[2]) * 0.5;
@@ -71,7 +71,7 @@ int orc_bbox(size_t n, const double *x, const double *y, const double *z,
 
 /* -------------------------------------------------------------- morton -- */
 
-/* morton.cu:168-177 */
+/* morton.cu:119-128 */
 static uint32_t expand_bits(uint32_t v) {
   uint32_t x = v & 0x000003FFu;
   x = (x | (x << 16)) & 0x030000FFu;
@@ -81,7 +81,7 @@ static uint32_t expand_bits(uint32_t v) {
   return x;
 }
 
-/* morton.cu:147-166: normalise against the cube, scale by the 1024-cell
+/* morton.cu:98-117: normalise against the cube, scale by the 1024-cell
  * grid, clamp to [0, 1023] and truncate. */
 static uint32_t quantise(double a, double centre, double side) {
   const double lower = centre - side / 2.0;
@@ -93,7 +93,7 @@ static uint32_t quantise(double a, double centre, double side) {
 
 /* Stable LSD radix sort of (key, value) pairs over all 32 key bits: the
  * result equals std::stable_sort / thrust::stable_sort_by_key
- * (morton.cu:270-273). */
+ * (morton.cu:221-224). */
 static void stable_sort_pairs(size_t n, uint32_t *keys, uint32_t *vals) {
   uint32_t *k2 = (uint32_t *)malloc(n * sizeof(uint32_t));
   uint32_t *v2 = (uint32_t *)malloc(n * sizeof(uint32_t));
@@ -118,9 +118,9 @@ static void stable_sort_pairs(size_t n, uint32_t *keys, uint32_t *vals) {
 
 int orc_morton(size_t n, const double *x, const double *y, const double *z,
                const double box[4], uint32_t *keys, uint32_t *idx) {
-  /* morton.cu:83-109 */
+  /* morton.cu:34-60 */
   if (n == 0 || !x || !y || !z) return ORC_EINVAL;
-  /* morton.cu:218-219 */
+  /* morton.cu:167-170 */
   if (!isfinite(box[0]) || !isfinite(box[1]) || !isfinite(box[2]) ||
       !isfinite(box[3]) || box[3] <= 0.0)
     return ORC_EINVAL;
@@ -128,9 +128,9 @@ int orc_morton(size_t n, const double *x, const double *y, const double *z,
     const uint32_t qx = quantise(x[i], box[0], box[3]);
     const uint32_t qy = quantise(y[i], box[1], box[3]);
     const uint32_t qz = quantise(z[i], box[2], box[3]);
-    /* morton.cu:185-187 */
+    /* morton.cu:130-139 */
     keys[i] = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
-    idx[i] = (uint32_t)i; /* morton.cu:214 */
+    idx[i] = (uint32_t)i; /* morton.cu:165 */
   }
   stable_sort_pairs(n, keys, idx);
   return ORC_OK;
@@ -140,10 +140,10 @@ int orc_morton(size_t n, const double *x, const double *y, const double *z,
 
 int orc_leaf_groups(int n, const uint32_t *sorted_keys, uint32_t *uniq,
                     int *first, int *count) {
-  /* morton_leaf_groups.cu:107-114 */
+  /* morton_leaf_groups.cu:60-70 */
   if (n <= 0 || !sorted_keys) return ORC_EINVAL;
   /* cub::DeviceRunLengthEncode::Encode + cub::DeviceScan::ExclusiveSum
-   * (morton_leaf_groups.cu:126-145). */
+   * (morton_leaf_groups.cu:76-98). */
   int g = 0;
   for (int i = 0; i < n; ++i) {
     if (i == 0 || sorted_keys[i] != sorted_keys[i - 1]) {
@@ -231,7 +231,7 @@ int orc_radix_tree(int n, const uint32_t *keys, int *left, int *right,
 
 /* --------------------------------------------------------------- plan -- */
 
-/* radix_to_octree.cu:124-138 */
+/* radix_to_octree.cu:54-68 */
 static int octree_level_of(int n_leaves, const int *plen, int r) {
   const int prefix = (r < n_leaves) ? MORTON_SPATIAL_BITS
                                     : plen[r - n_leaves] - MORTON_PADDING_BITS;
@@ -250,7 +250,7 @@ int orc_octree_plan(int n_leaves, const uint32_t *uniq, const int *parent,
     count[r] = 0;                      \
     continue;                          \
   } while (0)
-  /* radix_to_octree.cu:140-215 */
+  /* radix_to_octree.cu:70-145 */
   for (int r = 0; r < nr; ++r) {
     if (r < n_leaves) {
       if ((uniq[r] & ~MORTON_SPATIAL_MASK) != 0u) PLAN_FAIL(1);
@@ -273,7 +273,7 @@ int orc_octree_plan(int n_leaves, const uint32_t *uniq, const int *parent,
   }
 #undef PLAN_FAIL
   if (err) return err;
-  /* radix_to_octree.cu:291-313 */
+  /* radix_to_octree.cu:221-243 */
   long long running = 0;
   for (int r = 0; r < nr; ++r) {
     offset[r] = (int)running;
@@ -285,7 +285,7 @@ int orc_octree_plan(int n_leaves, const uint32_t *uniq, const int *parent,
 
 /* ------------------------------------------------------------ octree -- */
 
-/* octree_builder.cu:237-254 */
+/* octree_builder.cu:49-85 */
 static uint32_t prefix_at_level(uint32_t key, int lvl) {
   if (lvl == 0) return 0u;
   const int rem = MORTON_SPATIAL_BITS - lvl * MORTON_DIMS;
@@ -302,7 +302,7 @@ int orc_octree_build(int n_leaves, const uint32_t *uniq, const int *gfirst,
                      int *level, uint32_t *prefix, int *first, int *count) {
   const int nr = 2 * n_leaves - 1;
   if (m <= 0) return ORC_EINVAL;
-  /* octree_builder.cu:476-509 */
+  /* octree_builder.cu:288-321 */
   for (int i = 0; i < 8 * m; ++i) children[i] = -1;
   for (int i = 0; i < m; ++i) {
     parent[i] = -1;
@@ -319,7 +319,7 @@ int orc_octree_build(int n_leaves, const uint32_t *uniq, const int *gfirst,
     if (err == 0) err = (code); \
     goto next_radix;            \
   } while (0)
-  /* octree_builder.cu:275-412 */
+  /* octree_builder.cu:87-224 */
   for (int r = 0; r < nr; ++r) {
     const int cnt = plan_count[r];
     const int node_level = plan_level[r];
@@ -439,12 +439,12 @@ int orc_octree_mass(int m, int n, const int *children, const int *parent,
                     const double *pz, double *mass, double *comx,
                     double *comy, double *comz, int *child_count) {
   (void)parent;
-  /* octree_physics.cu:474-482: cleared first */
+  /* octree_physics.cu:302-310: cleared first */
   for (int i = 0; i < m; ++i) {
     mass[i] = comx[i] = comy[i] = comz[i] = 0.0;
     child_count[i] = 0;
   }
-  /* octree_physics.cu:236-265 */
+  /* octree_physics.cu:64-93 */
   int err = 0;
   for (int node = 0; node < m; ++node) {
     int c = 0;
@@ -463,7 +463,7 @@ int orc_octree_mass(int m, int n, const int *children, const int *parent,
     if (count[node] > 0 && c != 0 && !err) err = 4;
   }
   if (err) return err;
-  /* octree_physics.cu:267-326: occupied leaves summed in sorted order */
+  /* octree_physics.cu:95-154: occupied leaves summed in sorted order */
   for (int node = 0; node < m; ++node) {
     const int cnt = count[node];
     if (cnt <= 0) continue;
@@ -487,7 +487,7 @@ int orc_octree_mass(int m, int n, const int *children, const int *parent,
       comz[node] = wz * inv;
     }
   }
-  /* octree_physics.cu:328-417: the last arriving child sums the children in
+  /* octree_physics.cu:156-245: the last arriving child sums the children in
    * octant order 0..7, so a parent is combined only after every child.  A
    * reversed breadth-first order from the root gives the same dependency
    * order on the CPU. */
@@ -536,7 +536,7 @@ typedef struct {
   const double *mass, *comx, *comy, *comz, *cx, *cy, *cz, *half;
 } octree_view;
 
-/* barnes_hut.cu:76-100: returns 0 on success, 6 on a singular interaction. */
+/* barnes_hut.cu:56-80: returns 0 on success, 6 on a singular interaction. */
 static int point_mass(double tx, double ty, double tz, double sx, double sy,
                       double sz, double sm, double g, double soft2, double *ax,
                       double *ay, double *az) {
@@ -553,7 +553,7 @@ static int point_mass(double tx, double ty, double tz, double sx, double sy,
   return 0;
 }
 
-/* barnes_hut.cu:110-132 */
+/* barnes_hut.cu:90-112 */
 static int first_child(const octree_view *t, int node, int *err) {
   for (int o = 7; o >= 0; --o) {
     const int c = t->children[node * 8 + o];
@@ -568,7 +568,7 @@ static int first_child(const octree_view *t, int node, int *err) {
   return -2;
 }
 
-/* barnes_hut.cu:135-182 */
+/* barnes_hut.cu:115-162 */
 static int next_node(const octree_view *t, int node, int *err) {
   while (node != 0) {
     const int p = t->parent[node];
@@ -596,7 +596,7 @@ static int next_node(const octree_view *t, int node, int *err) {
   return -1;
 }
 
-/* barnes_hut.cu:184-342, one target. Returns the device error code (0 ok). */
+/* barnes_hut.cu:164-322, one target. Returns the device error code (0 ok). */
 static int traverse_one(const octree_view *t, const uint32_t *idx,
                         const double *pm, const double *px, const double *py,
                         const double *pz, int morton_ordered, int sorted_target,
@@ -686,7 +686,7 @@ int orc_bh_accel(int m, int n, const int *children, const int *parent,
                  int morton_ordered, double theta, double soft, double g,
                  double *ax, double *ay, double *az, int n_threads,
                  int64_t *interactions) {
-  /* barnes_hut.cu:349-383 */
+  /* barnes_hut.cu:325-391 */
   if (n <= 0 || m <= 0) return ORC_EINVAL;
   if (!isfinite(theta) || theta < 0.0) return ORC_EINVAL;
   if (!isfinite(soft) || soft < 0.0) return ORC_EINVAL;
@@ -746,7 +746,7 @@ void orc_direct_accel(int n, const double *pm, const double *px,
 void orc_kick_drift(size_t n, double *x, double *y, double *z, double *vx,
                     double *vy, double *vz, const double *ax, const double *ay,
                     const double *az, double dt) {
-  const double hdt = 0.5 * dt; /* integrator.cu:64 */
+  const double hdt = 0.5 * dt; /* integrator.cu:58 */
   for (size_t i = 0; i < n; ++i) {
     vx[i] = fma(hdt, ax[i], vx[i]);
     vy[i] = fma(hdt, ay[i], vy[i]);
@@ -759,7 +759,7 @@ void orc_kick_drift(size_t n, double *x, double *y, double *z, double *vx,
 
 void orc_kick(size_t n, double *vx, double *vy, double *vz, const double *ax,
               const double *ay, const double *az, double dt) {
-  const double hdt = 0.5 * dt; /* integrator.cu:99 */
+  const double hdt = 0.5 * dt; /* integrator.cu:93 */
   for (size_t i = 0; i < n; ++i) {
     vx[i] = fma(hdt, ax[i], vx[i]);
     vy[i] = fma(hdt, ay[i], vy[i]);
@@ -804,7 +804,7 @@ int orc_pipeline(size_t n, const double *m, const double *x, const double *y,
   if (st) return 400 + st;
   if (!o->ax) return 0;
   /* simulation.cu:34-58: gather into Morton order, then traverse with
-   * BarnesHutParticleOrder::morton (simulation.cpp:398-414). */
+   * BarnesHutParticleOrder::morton (simulation.cpp:182-198). */
   double *gm = (double *)malloc(4 * n * sizeof(double));
   double *gx = gm + n, *gy = gm + 2 * n, *gz = gm + 3 * n;
   for (size_t s = 0; s < n; ++s) {

@@ -37,15 +37,15 @@ enum {
   ORC_ECAP = -3      /* caller buffer too small */
 };
 
-/* globalbounding.cu:130-180 -- out = {centre_x, centre_y, centre_z, side}. */
+/* globalbounding.cu:94-144 -- out = {centre_x, centre_y, centre_z, side}. */
 int orc_bbox(size_t n, const double *x, const double *y, const double *z,
              double out[4]);
 
-/* morton.cu:147-188 + 209-274 -- keys and the stable (key, index) sort. */
+/* morton.cu:98-139,160-219 + 160-225 -- keys and the stable (key, index) sort. */
 int orc_morton(size_t n, const double *x, const double *y, const double *z,
                const double box[4], uint32_t *keys, uint32_t *idx);
 
-/* morton_leaf_groups.cu:105-150 -- run-length encode + exclusive scan.
+/* morton_leaf_groups.cu:58-103 -- run-length encode + exclusive scan.
  * Returns G (>0) or a negative status. */
 int orc_leaf_groups(int n, const uint32_t *sorted_keys, uint32_t *uniq,
                     int *first, int *count);
@@ -55,14 +55,14 @@ int orc_leaf_groups(int n, const uint32_t *sorted_keys, uint32_t *uniq,
 int orc_radix_tree(int n, const uint32_t *keys, int *left, int *right,
                    int *rfirst, int *rlast, int *plen, int *parent);
 
-/* radix_to_octree.cu:124-215 + 244-314 -- per radix node octree level, edge
+/* radix_to_octree.cu:54-145 + 174-243 -- per radix node octree level, edge
  * node count and their exclusive scan.  *n_octree receives 1 + sum.
  * Returns 0 or the reference's plan error code (1..4). */
 int orc_octree_plan(int n_leaves, const uint32_t *uniq, const int *parent,
                     const int *plen, int *level, int *count, int *offset,
                     int *n_octree);
 
-/* octree_builder.cu:237-412 + 442-550 -- materialise the sparse octree.
+/* octree_builder.cu:49-362 + 254-362 -- materialise the sparse octree.
  * children has 8*m entries. Returns 0 or construction error code (1..7). */
 int orc_octree_build(int n_leaves, const uint32_t *uniq, const int *gfirst,
                      const int *gcount, const int *rparent, const int *rfirst,
@@ -75,7 +75,7 @@ int orc_octree_geometry(int m, const int *level, const uint32_t *prefix,
                         const double box[4], double *cx, double *cy,
                         double *cz, double *half);
 
-/* octree_physics.cu:236-417 -- childCount, leaf mass/COM in sorted order,
+/* octree_physics.cu:64-337 -- childCount, leaf mass/COM in sorted order,
  * internal mass/COM summed in octant order 0..7. */
 int orc_octree_mass(int m, int n, const int *children, const int *parent,
                     const int *first, const int *count, const uint32_t *idx,
@@ -83,11 +83,11 @@ int orc_octree_mass(int m, int n, const int *children, const int *parent,
                     const double *pz, double *mass, double *comx,
                     double *comy, double *comz, int *child_count);
 
-/* barnes_hut.cu:76-342 -- per-target stackless traversal, children visited
+/* barnes_hut.cu:56-322 -- per-target stackless traversal, children visited
  * 7 -> 0.  Particle arrays are in original order (morton_ordered = 0) or
  * already gathered into Morton order (morton_ordered = 1); accelerations are
  * written at the original index.  theta/soft/g validated as
- * barnes_hut.cu:376-383.  n_threads <= 0 uses every available core.
+ * barnes_hut.cu:355-363.  n_threads <= 0 uses every available core.
  * interactions (may be NULL) receives the total count of monopole and
  * leaf-pair interactions. */
 int orc_bh_accel(int m, int n, const int *children, const int *parent,
@@ -108,7 +108,7 @@ void orc_direct_accel(int n, const double *pm, const double *px,
                       const int *targets, double g, double soft, double *ax,
                       double *ay, double *az, int n_threads);
 
-/* integrator.cu:57-112 */
+/* integrator.cu:51-106 */
 void orc_kick_drift(size_t n, double *x, double *y, double *z, double *vx,
                     double *vy, double *vz, const double *ax, const double *ay,
                     const double *az, double dt);
@@ -135,7 +135,7 @@ typedef struct {
   int64_t interactions;
 } orc_pipeline_out;
 
-/* simulation.cpp:353-414 -- rebuild the spatial structure from positions and
+/* simulation.cpp:137-198 -- rebuild the spatial structure from positions and
  * (if ax != NULL) evaluate Barnes-Hut accelerations with Morton-gathered
  * particle data.  Returns 0 or a status (negative host error, or 100*stage +
  * device code with stage 1 plan, 2 octree, 3 geometry, 4 physics,
@@ -144,7 +144,7 @@ int orc_pipeline(size_t n, const double *m, const double *x, const double *y,
                  const double *z, double theta, double soft, double g,
                  int n_threads, orc_pipeline_out *out);
 
-/* simulation.cpp:294-343 -- initialize() then `steps` calls of step():
+/* simulation.cpp:78-127 -- initialize() then `steps` calls of step():
  * KD, rebuild, force, K.  State arrays are updated in place; a (3n) holds the
  * last accelerations on return. */
 int orc_simulate(size_t n, const double *m, double *x, double *y, double *z,

@@ -8,12 +8,12 @@
 // tests and bench.py's reference arm load it.
 //
 // The call sequence replays the reference's own pipeline:
-//   Simulation::rebuildSpatialStructure   (src/simulation.cpp:353-396)
-//   Simulation::computeAccelerations      (src/simulation.cpp:398-414)
-//   Simulation::initialize / step         (src/simulation.cpp:294-335)
+//   Simulation::rebuildSpatialStructure   (src/simulation.cpp:137-180)
+//   Simulation::computeAccelerations      (src/simulation.cpp:182-198)
+//   Simulation::initialize / step         (src/simulation.cpp:78-119)
 // with an explicit gravitational constant, as the reference's accuracy test
 // does (tests/integration/cuda/barnes_hut_accuracy_test.cu:404-711), because
-// Simulation itself hard-codes the SI value (src/simulation.cpp:412).
+// Simulation itself hard-codes the SI value (src/simulation.cpp:196).
 #include <cuda_runtime.h>
 #include <thrust/device_vector.h>
 
@@ -65,7 +65,7 @@ struct Spatial {
   }
 };
 
-// src/simulation.cpp:353-381
+// src/simulation.cpp:137-165
 void rebuild(Spatial &s, const Bbox &box, const MortonKeys &morton,
              const double *dm, const double *dx, const double *dy,
              const double *dz, int n) {
@@ -84,7 +84,7 @@ void rebuild(Spatial &s, const Bbox &box, const MortonKeys &morton,
                                    dx, dy, dz);
 }
 
-// src/simulation.cpp:398-414 with an explicit G.
+// src/simulation.cpp:182-198 with an explicit G.
 void accelerations(nbody::detail::SimulationDeviceState &state,
                    const Octree &octree, const MortonKeys &morton,
                    const double *dm, const double *dx, const double *dy,
@@ -202,7 +202,7 @@ int ref_pipeline(std::size_t n, const double *m, const double *x,
   }
 }
 
-// initialize() then `steps` x step() of src/simulation.cpp:294-335 with an
+// initialize() then `steps` x step() of src/simulation.cpp:78-119 with an
 // explicit G.  State is updated in place; a receives the last acceleration.
 // step_ms (optional, `steps` entries) receives each step's CUDA-event time.
 int ref_simulate(std::size_t n, const double *m, double *x, double *y,

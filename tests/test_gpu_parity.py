@@ -135,7 +135,7 @@ def test_non_finite_positions_raise_domain_error(nbb_mod):
 
 
 def test_singular_interaction_reports_error(nbb_mod):
-    # barnes_hut.cu:88-89: coincident distinct particles with zero softening
+    # barnes_hut.cu:67-69: coincident distinct particles with zero softening
     p = _particles([1.0, 1.0, 1.0], [0.0, 0.0, 1.0], [0.0, 0.0, 1.0], [0.0, 0.0, 1.0])
     with pytest.raises(nbb_mod.DeviceError) as e:
         nbb_mod.compute_accelerations(p, 0.5, 0.0, 1.0)
