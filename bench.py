@@ -51,35 +51,44 @@ def workload_name(n):
 # ------------------------------------------------------------ clocks ---
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while running."""
+    """nvidia-smi samples of SM clock and throttle reasons, each stamped with
+    its arrival time on this host, so that a summary can cover exactly the
+    timed regions (the sampler starts well before them: nvidia-smi takes a
+    moment to produce its first line)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 20
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, csv line)
         self.thread = None
+        self.windows = []
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def __exit__(self, *exc):
+        time.sleep(2.5 * self.PERIOD_MS / 1000.0)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -89,10 +98,30 @@ class ClockSampler:
         if self.thread is not None:
             self.thread.join(timeout=2)
 
+    def window(self):
+        """Context manager marking one timed region."""
+        sampler = self
+
+        class _W:
+            def __enter__(self):
+                self.t0 = time.time()
+                return self
+
+            def __exit__(self, *exc):
+                sampler.windows.append((self.t0, time.time()))
+                return False
+
+        return _W()
+
     def summary(self):
+        """Median SM clock, max clock and throttle reasons of the samples that
+        arrived inside a timed region (one sampler period of slack after it)."""
+        slack = self.PERIOD_MS / 1000.0
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for t, line in self.lines:
+            if self.windows and not any(a <= t <= b + slack for a, b in self.windows):
+                continue
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -104,10 +133,11 @@ class ClockSampler:
             for name, val in zip(names, f[5:9]):
                 if val.lower() == "active":
                     reasons.add(name)
+        timed_s = sum(b - a for a, b in self.windows)
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0, "timed_s": timed_s}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "timed_s": timed_s, "period_ms": self.PERIOD_MS}
 
 
 # ------------------------------------------------------- distributed ---
@@ -205,20 +235,32 @@ def force_error(nbb, p, precision, targets):
             "targets": int(targets.size), "reference": "FP64 direct summation (GPU kernel)"}
 
 
-def cpu_baseline(p, budget_s=30.0):
-    """The oracle (CPU restatement of the reference pipeline) on this host:
-    one full rebuild + force evaluation over all targets (what a step costs,
-    KD/K are negligible), every core via OpenMP."""
+def cpu_baseline(p, samples=3):
+    """The oracle (CPU restatement of the reference pipeline) on this host,
+    every core via OpenMP: `samples` full steps -- kick-drift, rebuild, force
+    evaluation of every target, kick -- on a copy of the state; the value is
+    the median step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
 
     cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    pyoracle.pipeline(p.mass, p.x, p.y, p.z, theta=THETA, soft=EPS, g=G, n_threads=cores)
-    dt = time.perf_counter() - t0
+    m = np.ascontiguousarray(p.mass)
+    x, y, z, vx, vy, vz = (np.array(a, dtype=np.float64) for a in (p.x, p.y, p.z, p.vx, p.vy, p.vz))
+    a = pyoracle.pipeline(m, x, y, z, theta=THETA, soft=EPS, g=G, n_threads=cores)
+    ax, ay, az = a["ax"], a["ay"], a["az"]
+    times = []
+    for _ in range(samples):
+        t0 = time.perf_counter()
+        x, y, z, vx, vy, vz = pyoracle.kick_drift(x, y, z, vx, vy, vz, ax, ay, az, DT)
+        a = pyoracle.pipeline(m, x, y, z, theta=THETA, soft=EPS, g=G, n_threads=cores)
+        ax, ay, az = a["ax"], a["ay"], a["az"]
+        vx, vy, vz = pyoracle.kick(vx, vy, vz, ax, ay, az, DT)
+        times.append(time.perf_counter() - t0)
+    dt = statistics.median(times)
     return {"value": 1.0 / dt, "unit": "steps/s", "cores": cores, "kind": "port",
-            "sample": f"one full rebuild + force evaluation of all {len(p)} targets "
-                      f"({dt:.2f} s, OpenMP over targets)"}
+            "sample": f"median of {samples} full KDK steps of all {len(p)} particles (kick-drift, "
+                      f"rebuild, force evaluation of every target, kick; "
+                      f"{', '.join(f'{t:.2f}' for t in times)} s; OpenMP over targets)"}
 
 
 def run_nbb(args, rank, world, local):
@@ -233,61 +275,54 @@ def run_nbb(args, rank, world, local):
     stream = torch.cuda.Stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     results = {}
-    sampler = ClockSampler(local)
     sims = {}
     for name, prec in (("mixed", nbb.PRECISION_MIXED), ("fp64", nbb.PRECISION_FP64)):
         sim = nbb.Simulation(p, nbb.SimulationConfig(DT, THETA, EPS, G, precision=prec, device=local))
         sim.set_stream(stream.cuda_stream)
         sim.initialize()
         sims[name] = sim
-    for name, sim in sims.items():
-        for _ in range(args.warmup):
-            sim.step()
+    with ClockSampler(local) as sampler:
+        for name, sim in sims.items():
+            for _ in range(args.warmup):
+                sim.step()
+            torch.cuda.synchronize()
+            barrier(world)
+            torch.cuda.synchronize()
+            with sampler.window():
+                times, launches = time_steps(nbb, sim, torch, stream, flush, args.steps)
+                torch.cuda.synchronize()
+            barrier(world)
+            total_ms = max_over_ranks(sum(times), world)
+            stage_ms, st = sim.profile()
+            results[name] = {"ms_per_step": total_ms / args.steps, "step_ms": times, "launches": launches,
+                             "stages_ms": stage_ms, "interactions": st.interactions,
+                             "mac_tests": st.mac_tests, "stack_overflow": st.stack_overflow,
+                             "n_groups": st.n_groups, "n_octree_nodes": st.n_octree_nodes,
+                             "group_size": st.group_size}
+        # end to end through the public API: pinned host state in, step, state out
+        sim = sims["mixed"]
+        pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in p.arrays()]
+        hst = [t.numpy() for t in pin]
+        sim.upload(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6])
         torch.cuda.synchronize()
-        barrier(world)
-        torch.cuda.synchronize()
-        with (sampler if name == "mixed" else _Null()):
-            times, launches = time_steps(nbb, sim, torch, stream, flush, args.steps)
-        torch.cuda.synchronize()
-        barrier(world)
-        total_ms = max_over_ranks(sum(times), world)
-        stage_ms, st = sim.profile()
-        results[name] = {"ms_per_step": total_ms / args.steps, "step_ms": times, "launches": launches,
-                         "stages_ms": stage_ms, "interactions": st.interactions,
-                         "mac_tests": st.mac_tests, "stack_overflow": st.stack_overflow, "n_groups": st.n_groups,
-                         "n_octree_nodes": st.n_octree_nodes, "group_size": st.group_size}
-    # end to end through the public API: pinned host state in, step, state out
-    sim = sims["mixed"]
-    pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in p.arrays()]
-    hst = [t.numpy() for t in pin]
-    sim.upload(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6])
-    torch.cuda.synchronize()
-    e2e_times = []
-    for k in range(args.warmup + args.steps):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            e0.record(stream)
-        # upload, step and download in one call; the positions' copy back
-        # overlaps the rebuild and the walk
-        sim.step_host(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6],
-                      out=hst[1:])
-        with torch.cuda.stream(stream):
-            e1.record(stream)
-        e1.synchronize()
-        if k >= args.warmup:
-            e2e_times.append(e0.elapsed_time(e1))
+        e2e_times = []
+        for k in range(args.warmup + args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0.record(stream)
+            # upload, step and download in one call; the positions' copy back
+            # overlaps the rebuild and the walk
+            sim.step_host(mass=hst[0], x=hst[1], y=hst[2], z=hst[3], vx=hst[4], vy=hst[5], vz=hst[6],
+                          out=hst[1:])
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            if k >= args.warmup:
+                e2e_times.append(e0.elapsed_time(e1))
     e2e_ms = max_over_ranks(sum(e2e_times), world) / args.steps
     return p, results, e2e_ms, sampler.summary()
-
-
-class _Null:
-    def __enter__(self):
-        return self
-
-    def __exit__(self, *exc):
-        return False
 
 
 # Algorithmic bytes of the rebuild (the minimum each stage must move), per
@@ -304,20 +339,6 @@ def build_algorithmic_bytes(n, groups, nodes):
             + BUILD_BYTES_PER_RADIX_NODE * (2 * groups - 1) + BUILD_BYTES_PER_OCTREE_NODE * nodes)
 
 
-def profiled_traffic(kernel_file, variant=None):
-    """DRAM bytes per launch of a kernel from its committed ncu summary
-    (the line for `variant`, e.g. the warp group size, when given)."""
-    path = os.path.join(ROOT, "profiles", kernel_file)
-    key = "dram_bytes_per_launch" + (f"[{variant}]" if variant is not None else "") + ":"
-    try:
-        for line in open(path):
-            if line.startswith(key):
-                return int(line.split(":")[1])
-    except OSError:
-        pass
-    return None
-
-
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -325,6 +346,77 @@ def load_peaks():
             return json.load(f)
     except OSError:
         return {}
+
+
+PROFILE_CASES = ("step", "adjoint", "direct", "frozen", "diagnostics", "frame", "ensemble")
+
+
+def profile_run(args):
+    """One small, self-contained run of the kernels of one case, for ncu
+    captures (no timing, no JSON line).  Workload: the benchmark's Plummer
+    sphere at --n (theta 0.5, eps 0.01, dt 1e-3, G 1).
+
+      step         --steps graph-replayed steps of the --precision form (optional
+                   --group-size pins the mixed walk's target group size), then
+                   one diagnostic force evaluation with per-stage events
+      adjoint      a rollout of --adjoint steps (checkpoints every 32) and its
+                   backward pass for the loss sum(x_T) / n
+      direct       FP64 direct summation for 4096 seeded targets
+      frozen       frozen-structure replay of 4 perturbed copies over --steps steps
+      diagnostics  conserved quantities with the tree and all-pairs potentials
+      frame        one quantized frame of 100000 sampled particles
+      ensemble     --steps steps of 64 Plummer systems, N log-uniform in
+                   [1024, 131072], one segmented launch per stage
+    """
+    import nbb
+    from nbb import ics
+
+    prec = nbb.PRECISION_MIXED if args.precision == "mixed" else nbb.PRECISION_FP64
+    cfg = nbb.SimulationConfig(DT, THETA, EPS, G, precision=prec, group_size=args.group_size)
+    if args.profile == "ensemble":
+        ens = ics.plummer_ensemble(64, seed=3)
+        sim = nbb.EnsembleSimulation(ens, cfg)
+        sim.initialize()
+        sim.run(args.steps)
+        print("ensemble steps", args.steps, "particles", len(ens.particles))
+        return
+    p = ics.plummer(args.n, seed=0)
+    if args.profile == "direct":
+        rng = np.random.Generator(np.random.Philox(12345))
+        tg = np.sort(rng.choice(args.n, min(ERROR_TARGETS, args.n), replace=False)).astype(np.int32)
+        ax = nbb.compute_direct_accelerations(p.mass, p.x, p.y, p.z, G, EPS, targets=tg)[0]
+        print("direct", float(ax[0]))
+        return
+    if args.profile == "frozen":
+        rng = np.random.Generator(np.random.Philox(7))
+        copies = []
+        for _ in range(4):
+            q = ics.ParticleData(*(np.array(a) for a in p.arrays()))
+            q.x[rng.integers(0, args.n)] += 1e-6
+            copies.append(q)
+        out = nbb.frozen_rollout(p, cfg, copies, args.steps)
+        print("frozen copies", out.shape[0], float(out[0, 0, 0]))
+        return
+    sim = nbb.Simulation(p, cfg)
+    sim.initialize()
+    if args.profile == "adjoint":
+        sim.rollout(args.adjoint, 32)
+        gm, gx, gv = sim.backward(np.full((3, args.n), 1.0 / args.n))
+        print("backward done", float(gx[0, 0]))
+        return
+    if args.profile == "diagnostics":
+        d0 = sim.diagnostics(nbb.POTENTIAL_TREE)
+        d1 = sim.diagnostics(nbb.POTENTIAL_DIRECT) if args.n <= (1 << 17) else d0
+        print("energies", d0["total_energy"], d1["total_energy"])
+        return
+    if args.profile == "frame":
+        frame = sim.capture_frame(100000, sequence=1)
+        print("frame bytes", len(frame))
+        return
+    sim.run(args.steps)
+    stages, st = sim.profile()
+    print({k: round(v, 4) for k, v in stages.items()}, "interactions", st.interactions,
+          "mac_tests", st.mac_tests, "groups", st.n_groups, "nodes", st.n_octree_nodes)
 
 
 def main():
@@ -338,7 +430,15 @@ def main():
     ap.add_argument("--no-error", action="store_true")
     ap.add_argument("--workload", choices=["plummer", "disk", "blobs", "ensemble", "adjoint"],
                     default="plummer")
+    ap.add_argument("--profile", choices=PROFILE_CASES, default=None,
+                    help="run one small case of the kernels for an ncu capture (no timing)")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed", help="--profile step form")
+    ap.add_argument("--group-size", type=int, default=0, help="--profile: mixed walk group size (0 = tuned)")
+    ap.add_argument("--adjoint", type=int, default=4, help="--profile adjoint: rollout steps")
     args = ap.parse_args()
+    if args.profile:
+        profile_run(args)
+        return
     args.warmup = max(args.warmup, 3)
     if args.workload != "plummer":
         from nbb import workloads
@@ -400,9 +500,9 @@ def bench_nbb(args, rank, world, local):
     sm_mhz = clocks.get("sm_max_mhz") or 1965.0
     line["roofline"] = {"bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
                         "frac": achieved / peak32,
-                        "traffic": profiled_traffic("traverse_mixed_plummer_2e20.md", mixed["group_size"]),
-                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                          "launch (profiles/traverse_mixed_plummer_2e20.md)",
+                        # DRAM bytes per launch come from an ncu capture, which this timed run
+                        # does not take
+                        "traffic": None,
                         "kernel": "traverse_mixed_kernel",
                         "peak_source": "measured in this run: the larger of scalar FFMA "
                                        f"({peak32_scalar:.1f}) and packed FFMA2 ({peak32_packed:.1f}) "
@@ -414,7 +514,7 @@ def bench_nbb(args, rank, world, local):
     p_ach = 20.0 * plain["interactions"] / (ptrav * 1e-3) / 1e12
     line["plain_fp64"]["roofline"] = {"bound": "fp64", "achieved": p_ach, "peak": peak64,
                                       "unit": "TFLOP/s", "frac": p_ach / peak64,
-                                      "traffic": profiled_traffic("traverse_fp64_plummer_2e20.md"),
+                                      "traffic": None,
                                       "kernel": "traverse_fp64_kernel",
                                       "interactions_per_s": plain["interactions"] / (ptrav * 1e-3)}
     peaks = load_peaks()
