@@ -338,15 +338,23 @@ constexpr uint32_t kDigitMask = (1u << 30) - 1u;
 // round), so equal digits keep their input order: the result is the stable
 // order of thrust::stable_sort_by_key.  Tile prefixes per digit come from a
 // decoupled look-back over the tiles launched before it (tile ids are taken
-// from an atomic counter, so every predecessor is already running).
+// from an atomic counter, so every predecessor is already running).  The
+// ranked tile is first placed in shared memory in digit order, then written
+// out by consecutive threads: a digit's items of one tile land at consecutive
+// addresses, so the stores go out as runs instead of one scattered 8-byte
+// store per item.
 __global__ void __launch_bounds__(kSortThreads)
     onesweep_kernel(const unsigned long long *__restrict__ in,
                     unsigned long long *__restrict__ out, int n, int pass, int shift,
                     const uint32_t *__restrict__ digit_offsets,
                     uint32_t *status, DevScalars *sc) {
   constexpr int kWarps = kSortThreads / 32;
+  static_assert(kSortThreads == 256, "one thread per digit");
   __shared__ uint32_t whist[kWarps][256];
-  __shared__ uint32_t digit_base[256];
+  __shared__ uint32_t tile_excl[256];   // digit's first slot in the staged tile
+  __shared__ uint32_t digit_base[256];  // digit's first output position of this tile
+  __shared__ uint32_t warp_tot[kWarps];
+  __shared__ unsigned long long stage[kSortTile];
   __shared__ int s_tile;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid == 0) s_tile = (int)atomicAdd(&sc->tile_counter[pass], 1u);
@@ -378,7 +386,9 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncwarp();
   }
   __syncthreads();
-  if (tid < 256) {
+  {
+    // digit tid: offsets of the warps' runs, the tile's count, its place in
+    // the staged tile (exclusive scan over digits) and its output base
     uint32_t run = 0;
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
@@ -386,6 +396,12 @@ __global__ void __launch_bounds__(kSortThreads)
       whist[w][tid] = run;
       run += c;
     }
+    uint32_t inc = run;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (lane == 31) warp_tot[warp] = inc;
     uint32_t *my = status + (size_t)tile * 256 + tid;
     uint32_t prefix = 0;
     if (tile == 0) {
@@ -395,8 +411,8 @@ __global__ void __launch_bounds__(kSortThreads)
       int j = tile - 1;
       int spins = 0;
       while (j >= 0) {
-        const uint32_t s = ld_acquire_u32(status + (size_t)j * 256 + tid);
-        const uint32_t flag = s & ~kDigitMask;
+        const uint32_t st = ld_acquire_u32(status + (size_t)j * 256 + tid);
+        const uint32_t flag = st & ~kDigitMask;
         if (flag == 0u) {
           if (++spins > kSpinLimit) {
             record_error(sc, kStageSort, kCodeTimeout);
@@ -404,12 +420,16 @@ __global__ void __launch_bounds__(kSortThreads)
           }
           continue;
         }
-        prefix += s & kDigitMask;
+        prefix += st & kDigitMask;
         if (flag == kDigitFlagP) break;
         --j;
       }
       st_release_u32(my, kDigitFlagP | (prefix + run));
     }
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += warp_tot[w];
+    tile_excl[tid] = wbase + inc - run;
     digit_base[tid] = digit_offsets[pass * 256 + tid] + prefix;
   }
   __syncthreads();
@@ -418,12 +438,20 @@ __global__ void __launch_bounds__(kSortThreads)
     const int i = start + it * 32 + lane;
     if (i < n) {
       const uint32_t dig = (uint32_t)(key[it] >> shift) & 255u;
-      const uint32_t pos = digit_base[dig] + whist[warp][dig] + rank[it];
-      if (pos < (uint32_t)n) {
-        out[pos] = key[it];
-      } else {
-        record_error(sc, kStageSort, 1);
-      }
+      const uint32_t local = tile_excl[dig] + whist[warp][dig] + rank[it];
+      if (local < (uint32_t)kSortTile) stage[local] = key[it];
+    }
+  }
+  __syncthreads();
+  const int count = min(kSortTile, n - tile * kSortTile);
+  for (int j = tid; j < count; j += kSortThreads) {
+    const unsigned long long k = stage[j];
+    const uint32_t dig = (uint32_t)(k >> shift) & 255u;
+    const uint32_t pos = digit_base[dig] + ((uint32_t)j - tile_excl[dig]);
+    if (pos < (uint32_t)n) {
+      out[pos] = k;
+    } else {
+      record_error(sc, kStageSort, 1);
     }
   }
 }
@@ -901,52 +929,58 @@ __global__ void __launch_bounds__(kBlock) materialize_kernel(Workspace ws) {
 // Per node: cell centre / half size from the Morton prefix path
 // (octree_geometry.cu:56-102), child count (octree_physics.cu:64-93) and,
 // for occupied leaves, mass and centre of mass summed over the group's
-// particles in sorted order (octree_physics.cu:95-154).
+// particles in sorted order (octree_physics.cu:95-154).  The step runs both
+// parts in one pass; the function-level entry points (computeOctreeGeometry,
+// computeOctreeMassAndCenterOfMass) run one each.
+template <bool kGeometry, bool kPhysics>
 __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int m = sc->n_nodes;
   for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
-    const int level = ws.olevel[node];
-    if (level < 0 || level > ws.max_level) {
-      record_error(sc, kStageGeometry, 1);
-    } else {
-      const unsigned long long prefix = ws.oprefix[node];
-      const int kb = ws.key_bits;
-      bool valid = (prefix >> kb) == 0ull;
-      if (valid) {
-        if (level == 0) {
-          valid = prefix == 0ull;
-        } else {
-          const int rem = kb - level * kDims;
-          valid = (prefix & ((1ull << rem) - 1ull)) == 0ull;
-        }
-      }
-      if (!valid) {
-        record_error(sc, kStageGeometry, 2);
-      } else if (level < ws.sys_levels) {
-        // above the system roots of an ensemble: no cell, never visited
-        ws.cx[node] = 0.0;
-        ws.cy[node] = 0.0;
-        ws.cz[node] = 0.0;
-        ws.half[node] = 0.0;
+    if (kGeometry) {
+      const int level = ws.olevel[node];
+      if (level < 0 || level > ws.max_level) {
+        record_error(sc, kStageGeometry, 1);
       } else {
-        const double *box = ws.sys_box + 4 * (size_t)(prefix >> kSpatialBits);
-        double cx = box[0], cy = box[1], cz = box[2], h = __dmul_rn(box[3], 0.5);
-        for (int d = ws.sys_levels + 1; d <= level; ++d) {
-          const int oct = (int)((prefix >> (kb - d * kDims)) & 7ull);
-          const double ch = __dmul_rn(h, 0.5);
-          cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
-          cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
-          cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
-          h = ch;
+        const unsigned long long prefix = ws.oprefix[node];
+        const int kb = ws.key_bits;
+        bool valid = (prefix >> kb) == 0ull;
+        if (valid) {
+          if (level == 0) {
+            valid = prefix == 0ull;
+          } else {
+            const int rem = kb - level * kDims;
+            valid = (prefix & ((1ull << rem) - 1ull)) == 0ull;
+          }
         }
-        ws.cx[node] = cx;
-        ws.cy[node] = cy;
-        ws.cz[node] = cz;
-        ws.half[node] = h;
+        if (!valid) {
+          record_error(sc, kStageGeometry, 2);
+        } else if (level < ws.sys_levels) {
+          // above the system roots of an ensemble: no cell, never visited
+          ws.cx[node] = 0.0;
+          ws.cy[node] = 0.0;
+          ws.cz[node] = 0.0;
+          ws.half[node] = 0.0;
+        } else {
+          const double *box = ws.sys_box + 4 * (size_t)(prefix >> kSpatialBits);
+          double cx = box[0], cy = box[1], cz = box[2], h = __dmul_rn(box[3], 0.5);
+          for (int d = ws.sys_levels + 1; d <= level; ++d) {
+            const int oct = (int)((prefix >> (kb - d * kDims)) & 7ull);
+            const double ch = __dmul_rn(h, 0.5);
+            cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
+            cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
+            cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
+            h = ch;
+          }
+          ws.cx[node] = cx;
+          ws.cy[node] = cy;
+          ws.cz[node] = cz;
+          ws.half[node] = h;
+        }
       }
     }
+    if (!kPhysics) continue;
     const int4 *c4 = reinterpret_cast<const int4 *>(ws.children + (size_t)node * 8);
     const int4 a = c4[0], b = c4[1];
     const int ch[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
@@ -1350,6 +1384,41 @@ __global__ void __launch_bounds__(kBlock) split_pairs_kernel(const unsigned long
 
 // Reference-layout keys only (no particles): used by the function-level
 // topology entry points.
+// --------------------------------------- function-level stage helpers ---
+
+// 32-bit keys or prefixes to the workspace's 64-bit layout and back.
+__global__ void __launch_bounds__(kBlock) widen_u32_kernel(const uint32_t *in, int n, unsigned long long *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = in[i];
+}
+__global__ void __launch_bounds__(kBlock) narrow_u64_kernel(const unsigned long long *in, int n, uint32_t *out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (uint32_t)in[i];
+}
+// Group sizes from the first and last sorted index of each group.
+__global__ void __launch_bounds__(kBlock) group_counts_kernel(Workspace ws) {
+  const int g = ws.sc->error ? 0 : ws.sc->n_groups;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g; i += gridDim.x * blockDim.x)
+    ws.gcount[i] = ws.glast[i] - ws.gfirst[i] + 1;
+}
+// Sizes a stage works on, known to the caller (G groups, M octree nodes).
+__global__ void set_counts_kernel(DevScalars *sc, int g, int m) {
+  if (threadIdx.x == 0) {
+    sc->n_groups = g;
+    sc->n_nodes = m;
+  }
+}
+// Particle data gathered by the sorted indices, as octree_physics.cu:95-154
+// reads it (an index outside the particle array is its error 3).
+__global__ void __launch_bounds__(kBlock) gather_sorted_kernel(Workspace ws, const uint32_t *idx) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x) {
+    const uint32_t k = idx[i];
+    if (k >= (uint32_t)ws.n) {
+      record_error(ws.sc, kStagePhysics, 3);
+      continue;
+    }
+    ws.pm4[i] = make_double4(ws.x[k], ws.y[k], ws.z[k], ws.m[k]);
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x)
     ws.pairs_a[i] = ((unsigned long long)keys[i] << ws.pack_shift) | (unsigned)i;
@@ -1421,7 +1490,7 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   plan_kernel<<<ws.scan_tiles_r, kScanThreads, 0, s>>>(ws);
   octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
   materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
-  node_init_kernel<<<grid, kBlock, 0, s>>>(ws);
+  node_init_kernel<true, true><<<grid, kBlock, 0, s>>>(ws);
   level_bin_kernel<<<grid, kBlock, 0, s>>>(ws);
   for (int level = ws.max_level; level >= 0; --level)
     propagate_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
@@ -1495,6 +1564,100 @@ cudaError_t launch_topology(Workspace &ws, cudaStream_t s) {
   octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
   materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
   count_launches(4);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------- function-level stages ----
+// Each runs one stage of the build on a workspace whose arrays alias the
+// caller's (see the C ABI's function-level entry points).
+
+cudaError_t launch_bbox_only(Workspace &ws, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  reset_sys_kernel<<<1, 32, 0, s>>>(ws.sys_bb, ws.n_systems);
+  count_launches(2);
+  return launch_kd_bbox(ws, 0.0, 0, s);
+}
+
+cudaError_t launch_morton_sort_box(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  cudaError_t e = cudaMemsetAsync(ws.digit_hist, 0, sizeof(uint32_t) * kMaxSortPasses * 256, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)ws.sort_passes * ws.sort_tiles * 256, s);
+  if (e != cudaSuccess) return e;
+  e = launch_morton_sort_groups(ws, s, 1);
+  if (e != cudaSuccess) return e;
+  const unsigned long long *sorted = (ws.sort_passes & 1) ? ws.pairs_b : ws.pairs_a;
+  split_pairs_kernel<<<grid_for(ws, 4), kBlock, 0, s>>>(sorted, ws.n, ws.pack_shift, keys, idx);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_leaf_groups(Workspace &ws, const uint32_t *sorted_keys, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  cudaError_t e = cudaMemsetAsync(ws.scan_status, 0, sizeof(unsigned long long) * (size_t)ws.scan_tiles_n, s);
+  if (e != cudaSuccess) return e;
+  e = launch_groups_from_keys(ws, sorted_keys, s);
+  if (e != cudaSuccess) return e;
+  group_counts_kernel<<<grid_for(ws, 4), kBlock, 0, s>>>(ws);
+  count_launches(2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plan_only(Workspace &ws, int g, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  set_counts_kernel<<<1, 32, 0, s>>>(ws.sc, g, 0);
+  cudaError_t e = cudaMemsetAsync(ws.scan_status, 0,
+                                  sizeof(unsigned long long) * (size_t)(ws.scan_tiles_n + ws.scan_tiles_r), s);
+  if (e != cudaSuccess) return e;
+  plan_kernel<<<ws.scan_tiles_r, kScanThreads, 0, s>>>(ws);
+  count_launches(3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_octree_only(Workspace &ws, int g, int m, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  set_counts_kernel<<<1, 32, 0, s>>>(ws.sc, g, m);
+  const int grid = grid_for(ws, 8);
+  octree_clear_kernel<<<grid, kBlock, 0, s>>>(ws);
+  materialize_kernel<<<grid, kBlock, 0, s>>>(ws);
+  count_launches(4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_geometry_only(Workspace &ws, int m, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  set_counts_kernel<<<1, 32, 0, s>>>(ws.sc, 0, m);
+  node_init_kernel<true, false><<<grid_for(ws, 8), kBlock, 0, s>>>(ws);
+  count_launches(3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mass_only(Workspace &ws, const uint32_t *idx, int m, cudaStream_t s) {
+  reset_scalars_kernel<<<1, 32, 0, s>>>(ws.sc);
+  set_counts_kernel<<<1, 32, 0, s>>>(ws.sc, 0, m);
+  const int grid = grid_for(ws, 8);
+  gather_sorted_kernel<<<grid_for(ws, 4), kBlock, 0, s>>>(ws, idx);
+  node_init_kernel<false, true><<<grid, kBlock, 0, s>>>(ws);
+  level_bin_kernel<<<grid, kBlock, 0, s>>>(ws);
+  for (int level = ws.max_level; level >= 0; --level)
+    propagate_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
+  count_launches(6 + ws.max_level + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_widen_u32(const uint32_t *in, int n, unsigned long long *out, cudaStream_t s) {
+  int blocks = (n + kBlock - 1) / kBlock;
+  blocks = blocks < 1 ? 1 : (blocks > 4096 ? 4096 : blocks);
+  widen_u32_kernel<<<blocks, kBlock, 0, s>>>(in, n, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_narrow_u64(const unsigned long long *in, int n, uint32_t *out, cudaStream_t s) {
+  int blocks = (n + kBlock - 1) / kBlock;
+  blocks = blocks < 1 ? 1 : (blocks > 4096 ? 4096 : blocks);
+  narrow_u64_kernel<<<blocks, kBlock, 0, s>>>(in, n, out);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -1301,6 +1301,316 @@ int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right, int *rfir
   return ok();
 }
 
+
+}  // extern "C"
+
+// ------------------------------------------- function-level build stages ---
+
+namespace {
+
+// A workspace for one function-level stage: device scalars (zeroed), the
+// default stream, every other array aliased to the caller's or taken here.
+struct StageRun {
+  Workspace ws{};
+  Allocation al;
+  cudaStream_t s = nullptr;  // the default stream: synchronous as the reference
+  cudaError_t init(int n) {
+    ws.n = n;
+    ws.n_systems = 1;
+    ws.sys_levels = 0;
+    ws.key_bits = kSpatialBits;
+    ws.max_level = kMaxLevel;
+    ws.pack_shift = 64 - kSpatialBits;
+    ws.sort_passes = kSortPasses;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&ws.num_sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = al.get(ws.sc, 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ws.sc, 0, sizeof(DevScalars), s);
+    return e;
+  }
+};
+
+int read_box(const double *box, double out[4]) {
+  NBB_CUDA(cudaMemcpy(out, box, 4 * sizeof(double), cudaMemcpyDeviceToHost), "copy bounding box");
+  return ok();
+}
+
+bool box_valid(const double b[4]) {
+  return std::isfinite(b[0]) && std::isfinite(b[1]) && std::isfinite(b[2]) && std::isfinite(b[3]) && b[3] > 0.0;
+}
+
+int read_scalar(const int *p, int *out) {
+  NBB_CUDA(cudaMemcpy(out, p, sizeof(int), cudaMemcpyDeviceToHost), "copy device count");
+  return ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+int nbb_bbox(const double *x, const double *y, const double *z, size_t n, double *box) {
+  if (n == 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Cannot compute a bounding box for an empty particle set.");
+  if (n > (size_t)INT_MAX) return fail(NBB_ERR_OVERFLOW, "Particle count exceeds the tree representation");
+  if (!x || !y || !z || !box) return fail(NBB_ERR_INVALID_ARGUMENT, "Bounding box device pointers must not be null");
+  StageRun st;
+  NBB_CUDA(st.init((int)n), "bounding box set-up");
+  Workspace &ws = st.ws;
+  ws.x = const_cast<double *>(x);
+  ws.y = const_cast<double *>(y);
+  ws.z = const_cast<double *>(z);
+  NBB_CUDA(st.al.get(ws.sys_bb, 6), "bounding box set-up");
+  ws.sys_box = box;
+  NBB_CUDA(launch_bbox_only(ws, st.s), "Bbox::compute_box");
+  return check_device(ws, st.s);
+}
+
+int nbb_morton_keys(const double *x, const double *y, const double *z, size_t n, const double *box,
+                    uint32_t *keys, uint32_t *idx) {
+  // morton.cu:34-60 and :167-170
+  if (n == 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Cannot compute Morton keys for an empty particle set");
+  if (!x || !y || !z) return fail(NBB_ERR_INVALID_ARGUMENT, "Morton coordinate device pointers must not be null");
+  if (n > (size_t)INT_MAX) return fail(NBB_ERR_OVERFLOW, "Particle count exceeds the Morton index representation");
+  if (!box || !keys || !idx) return fail(NBB_ERR_INVALID_ARGUMENT, "Morton box and output device pointers must not be null");
+  double b[4];
+  int r = read_box(box, b);
+  if (r) return r;
+  if (!box_valid(b)) return fail(NBB_ERR_INVALID_ARGUMENT, "Morton bounding box is not valid");
+  StageRun st;
+  NBB_CUDA(st.init((int)n), "Morton set-up");
+  Workspace &ws = st.ws;
+  ws.x = const_cast<double *>(x);
+  ws.y = const_cast<double *>(y);
+  ws.z = const_cast<double *>(z);
+  ws.sys_box = const_cast<double *>(box);
+  ws.sort_tiles = ((int)n + kSortTile - 1) / kSortTile;
+  NBB_CUDA(st.al.get(ws.digit_hist, (size_t)kMaxSortPasses * 256), "Morton set-up");
+  NBB_CUDA(st.al.get(ws.sort_status, (size_t)ws.sort_passes * ws.sort_tiles * 256), "Morton set-up");
+  NBB_CUDA(st.al.get(ws.pairs_a, n), "Morton set-up");
+  NBB_CUDA(st.al.get(ws.pairs_b, n), "Morton set-up");
+  NBB_CUDA(launch_morton_sort_box(ws, keys, idx, st.s), "MortonKeys::build");
+  return check_device(ws, st.s);
+}
+
+int nbb_leaf_groups(const uint32_t *sorted_keys, int n, uint32_t *unique_keys, int *first, int *count,
+                    int *n_groups) {
+  // morton_leaf_groups.cu:60-70
+  if (n <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "buildMortonLeafGroups requires nParticles >= 1");
+  if (!sorted_keys) return fail(NBB_ERR_INVALID_ARGUMENT, "d_sortedKeys must not be null");
+  if (!unique_keys || !first || !count || !n_groups)
+    return fail(NBB_ERR_LOGIC, "MortonLeafGroups memory has not been allocated");
+  StageRun st;
+  NBB_CUDA(st.init(n), "leaf-group set-up");
+  Workspace &ws = st.ws;
+  ws.pack_shift = 32;  // caller keys may use all 32 bits
+  ws.scan_tiles_n = (n + kScanTile - 1) / kScanTile;
+  const size_t N = (size_t)n;
+  NBB_CUDA(st.al.get(ws.pairs_a, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.ukey, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.glast, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.keys, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.idx, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.psys, N), "leaf-group set-up");
+  NBB_CUDA(st.al.get(ws.scan_status, (size_t)ws.scan_tiles_n), "leaf-group set-up");
+  ws.uniq = unique_keys;
+  ws.gfirst = first;
+  ws.gcount = count;
+  NBB_CUDA(launch_leaf_groups(ws, sorted_keys, st.s), "buildMortonLeafGroups");
+  int r = check_device(ws, st.s);
+  if (r) return r;
+  r = read_scalar(&ws.sc->n_groups, n_groups);
+  if (r) return r;
+  if (*n_groups <= 0 || *n_groups > n)
+    return fail(NBB_ERR_DEVICE, "DeviceRunLengthEncode produced an invalid group count");
+  return ok();
+}
+
+int nbb_radix_tree_device(const uint32_t *keys, int n, int *left, int *right, int *rfirst, int *rlast, int *plen,
+                          int *parent) {
+  // tree_builder.cu:305-324
+  if (n <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "buildTree requires N >= 1");
+  if (!parent || (n > 1 && (!left || !right || !rfirst || !rlast || !plen)))
+    return fail(NBB_ERR_LOGIC, "Tree memory has not been allocated");
+  if (!keys) return fail(NBB_ERR_INVALID_ARGUMENT, "d_sortedKeys must not be null");
+  NBB_CUDA(launch_radix_tree_only(keys, n, left, right, rfirst, rlast, plen, parent, nullptr), "buildTreeKernel launch");
+  NBB_CUDA(cudaStreamSynchronize(nullptr), "buildTreeKernel execution");
+  return ok();
+}
+
+int nbb_octree_plan(const uint32_t *unique_keys, int n_groups, const int *plen, const int *parent, int *level,
+                    int *count, int *offset, int *n_octree_nodes) {
+  // radix_to_octree.cu:176-197
+  if (n_groups <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "The radix tree has no leaves");
+  if (!unique_keys) return fail(NBB_ERR_LOGIC, "Morton unique keys are not allocated");
+  if (!parent) return fail(NBB_ERR_LOGIC, "Radix-tree parent array is not allocated");
+  if (!plen && n_groups > 1) return fail(NBB_ERR_LOGIC, "Radix-tree prefix metadata is not allocated");
+  if (!level || !count || !offset || !n_octree_nodes)
+    return fail(NBB_ERR_LOGIC, "RadixToOctreePlan memory is not allocated");
+  StageRun st;
+  NBB_CUDA(st.init(n_groups), "plan set-up");
+  Workspace &ws = st.ws;
+  ws.cap_nodes = INT_MAX;  // the reference's bound: the count must fit in int
+  ws.scan_tiles_n = (n_groups + kScanTile - 1) / kScanTile;
+  ws.scan_tiles_r = (2 * n_groups - 1 + kScanTile - 1) / kScanTile;
+  NBB_CUDA(st.al.get(ws.ukey, (size_t)n_groups), "plan set-up");
+  NBB_CUDA(st.al.get(ws.scan_status, (size_t)(ws.scan_tiles_n + ws.scan_tiles_r)), "plan set-up");
+  NBB_CUDA(launch_widen_u32(unique_keys, n_groups, ws.ukey, st.s), "plan set-up");
+  ws.plen = const_cast<int *>(plen);
+  ws.rparent = const_cast<int *>(parent);
+  ws.plevel = level;
+  ws.pcount = count;
+  ws.poffset = offset;
+  NBB_CUDA(launch_plan_only(ws, n_groups, st.s), "computeRadixToOctreePlanKernel");
+  int r = check_device(ws, st.s);
+  if (r) return r;
+  return read_scalar(&ws.sc->n_nodes, n_octree_nodes);
+}
+
+int nbb_octree_topology(const uint32_t *unique_keys, const int *group_first, const int *group_count, int n_groups,
+                        const int *rfirst, const int *parent, const int *plan_level, const int *plan_count,
+                        const int *plan_offset, int n_nodes, int *children, int *octree_parent, int *octree_level,
+                        uint32_t *octree_prefix, int *first, int *count) {
+  // octree_builder.cu:256-286
+  if (n_groups <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Morton groups are empty");
+  if (!unique_keys || !group_first || !group_count) return fail(NBB_ERR_LOGIC, "Morton group arrays are not allocated");
+  if (n_nodes <= 0) return fail(NBB_ERR_INVALID_ARGUMENT, "Radix-to-octree plan has no octree nodes");
+  if (!children || !octree_parent || !octree_level || !octree_prefix || !first || !count)
+    return fail(NBB_ERR_LOGIC, "Octree topology memory is not allocated");
+  if (!parent) return fail(NBB_ERR_LOGIC, "Radix parent array is not allocated");
+  if (!rfirst && n_groups > 1) return fail(NBB_ERR_LOGIC, "Radix metadata is incomplete");
+  if (!plan_level || !plan_count || !plan_offset) return fail(NBB_ERR_LOGIC, "Radix-to-octree plan arrays are not allocated");
+  StageRun st;
+  NBB_CUDA(st.init(n_groups), "octree set-up");
+  Workspace &ws = st.ws;
+  const size_t M = (size_t)n_nodes;
+  ws.cap_nodes = n_nodes;
+  NBB_CUDA(st.al.get(ws.ukey, (size_t)n_groups), "octree set-up");
+  NBB_CUDA(st.al.get(ws.oprefix, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.child_count, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.subtree, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.preoff, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.psub, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.pfirst, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.mass, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.comx, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.comy, M), "octree set-up");
+  NBB_CUDA(st.al.get(ws.comz, M), "octree set-up");
+  NBB_CUDA(launch_widen_u32(unique_keys, n_groups, ws.ukey, st.s), "octree set-up");
+  ws.gfirst = const_cast<int *>(group_first);
+  ws.gcount = const_cast<int *>(group_count);
+  ws.rfirst = const_cast<int *>(rfirst);
+  ws.rparent = const_cast<int *>(parent);
+  ws.plevel = const_cast<int *>(plan_level);
+  ws.pcount = const_cast<int *>(plan_count);
+  ws.poffset = const_cast<int *>(plan_offset);
+  ws.children = children;
+  ws.oparent = octree_parent;
+  ws.olevel = octree_level;
+  ws.ofirst = first;
+  ws.ocount = count;
+  NBB_CUDA(launch_octree_only(ws, n_groups, n_nodes, st.s), "materializeSparseOctreeKernel");
+  NBB_CUDA(launch_narrow_u64(ws.oprefix, n_nodes, octree_prefix, st.s), "octree prefixes");
+  return check_device(ws, st.s);
+}
+
+int nbb_octree_geometry(int n_nodes, const int *level, const uint32_t *prefix, const double *box, double *cx,
+                        double *cy, double *cz, double *half) {
+  // octree_geometry.cu:139-152
+  if (n_nodes <= 0) return fail(NBB_ERR_LOGIC, "Octree topology is not valid");
+  if (!level || !prefix) return fail(NBB_ERR_LOGIC, "Octree topology arrays required for geometry are not allocated");
+  if (!cx || !cy || !cz || !half) return fail(NBB_ERR_LOGIC, "Octree geometry arrays are not allocated");
+  if (!box) return fail(NBB_ERR_INVALID_ARGUMENT, "Bounding box geometry is not valid");
+  double b[4];
+  int r = read_box(box, b);
+  if (r) return r;
+  if (!box_valid(b)) return fail(NBB_ERR_INVALID_ARGUMENT, "Bounding box geometry is not valid");
+  StageRun st;
+  NBB_CUDA(st.init(n_nodes), "geometry set-up");
+  Workspace &ws = st.ws;
+  NBB_CUDA(st.al.get(ws.oprefix, (size_t)n_nodes), "geometry set-up");
+  NBB_CUDA(launch_widen_u32(prefix, n_nodes, ws.oprefix, st.s), "geometry set-up");
+  ws.olevel = const_cast<int *>(level);
+  ws.sys_box = const_cast<double *>(box);
+  ws.cx = cx;
+  ws.cy = cy;
+  ws.cz = cz;
+  ws.half = half;
+  NBB_CUDA(launch_geometry_only(ws, n_nodes, st.s), "computeOctreeGeometryKernel");
+  return check_device(ws, st.s);
+}
+
+int nbb_octree_mass(int n_nodes, int n_particles, const int *children, const int *level, const int *first,
+                    const int *count, const uint32_t *sorted_indices, const double *mass, const double *x,
+                    const double *y, const double *z, int *child_count, double *node_mass, double *comx,
+                    double *comy, double *comz) {
+  // octree_physics.cu:283-314
+  if (n_nodes <= 0 || n_particles <= 0) return fail(NBB_ERR_LOGIC, "Octree topology is not valid");
+  if (!children || !level || !first || !count) return fail(NBB_ERR_LOGIC, "Octree topology arrays are not allocated");
+  if (!child_count || !node_mass || !comx || !comy || !comz)
+    return fail(NBB_ERR_LOGIC, "Octree physical arrays are not allocated");
+  if (!sorted_indices) return fail(NBB_ERR_INVALID_ARGUMENT, "d_sortedIndices must not be null");
+  if (!mass || !x || !y || !z) return fail(NBB_ERR_INVALID_ARGUMENT, "Particle arrays must not be null");
+  StageRun st;
+  NBB_CUDA(st.init(n_particles), "mass set-up");
+  Workspace &ws = st.ws;
+  const size_t M = (size_t)n_nodes;
+  ws.cap_nodes = node_capacity(n_particles, kMaxLevel);
+  NBB_CUDA(st.al.get(ws.pm4, (size_t)n_particles), "mass set-up");
+  NBB_CUDA(st.al.get(ws.subtree, M), "mass set-up");
+  NBB_CUDA(st.al.get(ws.preoff, M), "mass set-up");
+  NBB_CUDA(st.al.get(ws.psub, M), "mass set-up");
+  NBB_CUDA(st.al.get(ws.pfirst, M), "mass set-up");
+  NBB_CUDA(st.al.get(ws.by_level, (size_t)ws.cap_nodes), "mass set-up");
+  NBB_CUDA(cudaMemsetAsync(ws.subtree, 0, M * sizeof(int), st.s), "mass set-up");
+  NBB_CUDA(cudaMemsetAsync(ws.psub, 0, M * sizeof(int), st.s), "mass set-up");
+  NBB_CUDA(cudaMemsetAsync(ws.pfirst, 0x7F, M * sizeof(int), st.s), "mass set-up");
+  // octree_physics.cu:302-310: node masses and centres of mass start at zero
+  NBB_CUDA(cudaMemsetAsync(node_mass, 0, M * sizeof(double), st.s), "clear octree.mass");
+  NBB_CUDA(cudaMemsetAsync(comx, 0, M * sizeof(double), st.s), "clear octree.comX");
+  NBB_CUDA(cudaMemsetAsync(comy, 0, M * sizeof(double), st.s), "clear octree.comY");
+  NBB_CUDA(cudaMemsetAsync(comz, 0, M * sizeof(double), st.s), "clear octree.comZ");
+  NBB_CUDA(cudaMemsetAsync(child_count, 0, M * sizeof(int), st.s), "clear octree.childCount");
+  ws.m = const_cast<double *>(mass);
+  ws.x = const_cast<double *>(x);
+  ws.y = const_cast<double *>(y);
+  ws.z = const_cast<double *>(z);
+  ws.children = const_cast<int *>(children);
+  ws.olevel = const_cast<int *>(level);
+  ws.ofirst = const_cast<int *>(first);
+  ws.ocount = const_cast<int *>(count);
+  ws.child_count = child_count;
+  ws.mass = node_mass;
+  ws.comx = comx;
+  ws.comy = comy;
+  ws.comz = comz;
+  NBB_CUDA(launch_mass_only(ws, sorted_indices, n_nodes, st.s), "computeOctreeMassAndCenterOfMass");
+  return check_device(ws, st.s);
+}
+
+int nbb_device_alloc(void **ptr, size_t bytes) {
+  if (!ptr) return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_device_alloc: null output pointer");
+  *ptr = nullptr;
+  if (bytes == 0) return ok();
+  NBB_CUDA(cudaMalloc(ptr, bytes), "cudaMalloc");
+  return ok();
+}
+
+int nbb_device_free(void *ptr) {
+  if (ptr) NBB_CUDA(cudaFree(ptr), "cudaFree");
+  return ok();
+}
+
+int nbb_memcpy(void *dst, const void *src, size_t bytes, int kind) {
+  if (bytes == 0) return ok();
+  if (!dst || !src) return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_memcpy: null pointer");
+  const cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice
+                           : kind == 1 ? cudaMemcpyDeviceToHost
+                           : kind == 2 ? cudaMemcpyDeviceToDevice : cudaMemcpyDefault;
+  if (kind < 0 || kind > 2) return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_memcpy: kind must be 0, 1 or 2");
+  NBB_CUDA(cudaMemcpy(dst, src, bytes, k), "cudaMemcpy");
+  return ok();
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------- adjoint ----

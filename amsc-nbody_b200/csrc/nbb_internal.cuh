@@ -308,6 +308,22 @@ cudaError_t launch_groups_from_keys(Workspace &ws, const uint32_t *sorted_keys,
 // Topology stages only (Karras .. materialise) for caller keys.
 cudaError_t launch_topology(Workspace &ws, cudaStream_t s);
 
+// Function-level stages (one reference build function each) on workspaces
+// whose arrays alias the caller's: the box alone; keys and the sort against
+// the box in ws.sys_box; leaf groups of caller keys (with their sizes); the
+// plan of g groups; the octree of g groups and m nodes; cell geometry of m
+// nodes; child counts, leaf and internal mass / centre of mass of m nodes
+// from particles gathered by idx.
+cudaError_t launch_bbox_only(Workspace &ws, cudaStream_t s);
+cudaError_t launch_morton_sort_box(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s);
+cudaError_t launch_leaf_groups(Workspace &ws, const uint32_t *sorted_keys, cudaStream_t s);
+cudaError_t launch_plan_only(Workspace &ws, int g, cudaStream_t s);
+cudaError_t launch_octree_only(Workspace &ws, int g, int m, cudaStream_t s);
+cudaError_t launch_geometry_only(Workspace &ws, int m, cudaStream_t s);
+cudaError_t launch_mass_only(Workspace &ws, const uint32_t *idx, int m, cudaStream_t s);
+cudaError_t launch_widen_u32(const uint32_t *in, int n, unsigned long long *out, cudaStream_t s);
+cudaError_t launch_narrow_u64(const unsigned long long *in, int n, uint32_t *out, cudaStream_t s);
+
 // Reverse-mode buffers of one frozen-structure force evaluation.  The
 // accelerations cotangent is coef * (gvx, gvy, gvz); gx / gy / gz / gm
 // accumulate; gv += dt_v * gx afterwards when dt_v != 0.

@@ -258,6 +258,78 @@ int nbb_octree_from_keys(const uint32_t *sorted_keys, int n,
 int nbb_radix_tree(const uint32_t *keys, int n, int *left, int *right,
                    int *rfirst, int *rlast, int *plen, int *parent);
 
+/* ----------------------------------------- function-level build stages ----
+ * One entry point per build function of the reference, on caller DEVICE
+ * arrays laid out as the reference's structures (src/morton.hpp,
+ * src/morton_leaf_groups.hpp:8-41, src/tree_types.hpp:48-109,
+ * src/radix_to_octree.hpp:31-65, src/octree_types.hpp:73-178).  Each call is
+ * synchronous on the default stream, as the reference's are, and reports the
+ * reference's errors (messages and exception classes of the same stage). */
+
+/* Bbox::compute_box (gpu/cuda_kernels/globalbounding.cu:94-144): box receives
+ * {centre x, y, z, side} in device memory. */
+int nbb_bbox(const double *x, const double *y, const double *z, size_t n,
+             double *box);
+
+/* MortonKeys::build (gpu/cuda_kernels/morton.cu:160-225): keys of the
+ * positions against the device box and their stable ascending sort with the
+ * particle indices. */
+int nbb_morton_keys(const double *x, const double *y, const double *z,
+                    size_t n, const double *box, uint32_t *keys,
+                    uint32_t *idx);
+
+/* buildMortonLeafGroups (gpu/cuda_kernels/morton_leaf_groups.cu:58-103):
+ * unique keys, first sorted index and size of every run of equal keys;
+ * *n_groups (host) receives G. */
+int nbb_leaf_groups(const uint32_t *sorted_keys, int n, uint32_t *unique_keys,
+                    int *first, int *count, int *n_groups);
+
+/* buildTree (gpu/cuda_kernels/tree_builder.cu:303-352) on device keys:
+ * left..plen n-1 entries (NULL allowed for n = 1), parent 2n-1. */
+int nbb_radix_tree_device(const uint32_t *keys, int n, int *left, int *right,
+                          int *rfirst, int *rlast, int *plen, int *parent);
+
+/* buildRadixToOctreePlan (gpu/cuda_kernels/radix_to_octree.cu:174-244) for a
+ * tree over n_groups unique keys: level, count and offset per radix node
+ * (2 n_groups - 1); *n_octree_nodes (host) receives M. */
+int nbb_octree_plan(const uint32_t *unique_keys, int n_groups, const int *plen,
+                    const int *parent, int *level, int *count, int *offset,
+                    int *n_octree_nodes);
+
+/* buildSparseOctreeTopology (gpu/cuda_kernels/octree_builder.cu:254-362):
+ * the M-node octree of a radix tree, its leaf groups and plan. */
+int nbb_octree_topology(const uint32_t *unique_keys, const int *group_first,
+                        const int *group_count, int n_groups,
+                        const int *rfirst, const int *parent,
+                        const int *plan_level, const int *plan_count,
+                        const int *plan_offset, int n_nodes, int *children,
+                        int *octree_parent, int *octree_level,
+                        uint32_t *octree_prefix, int *first, int *count);
+
+/* computeOctreeGeometry (gpu/cuda_kernels/octree_geometry.cu:137-173): cell
+ * centre and half size of every node from its level and Morton prefix and
+ * the device box. */
+int nbb_octree_geometry(int n_nodes, const int *level, const uint32_t *prefix,
+                        const double *box, double *cx, double *cy, double *cz,
+                        double *half);
+
+/* computeOctreeMassAndCenterOfMass (gpu/cuda_kernels/octree_physics.cu:
+ * 283-337): child counts, and mass and centre of mass of every node -- leaves
+ * over their particles in sorted order, internal nodes over their children in
+ * octant order -- for n_particles particles reached through sorted_indices. */
+int nbb_octree_mass(int n_nodes, int n_particles, const int *children,
+                    const int *level, const int *first, const int *count,
+                    const uint32_t *sorted_indices, const double *mass,
+                    const double *x, const double *y, const double *z,
+                    int *child_count, double *node_mass, double *comx,
+                    double *comy, double *comz);
+
+/* Device memory for the C++ layer's buffers (cudaMalloc / cudaFree /
+ * cudaMemcpy; kind 0 host to device, 1 device to host, 2 device to device). */
+int nbb_device_alloc(void **ptr, size_t bytes);
+int nbb_device_free(void *ptr);
+int nbb_memcpy(void *dst, const void *src, size_t bytes, int kind);
+
 /* Diagnostic: measured SIMT FMA throughput of the current device in TFLOP/s
  * (precision NBB_PRECISION_FP64, NBB_PRECISION_MIXED = scalar FP32, or 2 =
  * packed two-wide FP32), the roofline denominators of the traversal kernels. */

@@ -107,3 +107,77 @@ def test_cli_writes_frames(tmp_path, nbb_mod):
     with open(spool / snaps[-1], "rb") as f:
         h = frames.read_header(f.read())
     assert (h["version"], h["sequence"], h["simulation_step"], h["simulation_time"]) == (3, 3, 3, 0.75)
+
+
+def test_build_api_header_compiles(tmp_path):
+    # nbb_build.hpp with the reference's function-level names compiles as C++17
+    # without CUDA headers (its buffers go through the C ABI)
+    src = tmp_path / "t.cpp"
+    src.write_text('#include "nbb_build.hpp"\nint main() { Tree t; MortonLeafGroups g; return t.nLeaves + g.nGroups; }\n')
+    subprocess.check_call(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", *INC, str(src)])
+
+
+BUILD_API_FIELDS = ["box", "keys", "idx", "uniq", "gfirst", "gcount", "left", "right", "rfirst", "rlast", "plen",
+                    "rparent", "plan_level", "plan_count", "plan_offset", "children", "oparent", "olevel",
+                    "oprefix", "ofirst", "ocount", "child_count", "cx", "cy", "cz", "half", "mass", "comx",
+                    "comy", "comz"]
+BUILD_API_TYPES = {"box": "<f8", "keys": "<u4", "idx": "<u4", "uniq": "<u4", "oprefix": "<u4", "cx": "<f8",
+                   "cy": "<f8", "cz": "<f8", "half": "<f8", "mass": "<f8", "comx": "<f8", "comy": "<f8",
+                   "comz": "<f8"}
+BUILD_API_THETAS = (0.0, 0.3, 0.5, 0.7, 1.0)
+
+
+def _read_build_api_output(path):
+    import numpy as np
+
+    data = open(path, "rb").read()
+    pos, out = 0, {}
+
+    def take(dtype):
+        nonlocal pos
+        (count,) = struct.unpack_from("<Q", data, pos)
+        pos += 8
+        a = np.frombuffer(data, dtype=dtype, count=count, offset=pos).copy()
+        pos += a.nbytes
+        return a
+
+    for f in BUILD_API_FIELDS:
+        out[f] = take(BUILD_API_TYPES.get(f, "<i4"))
+    for theta in BUILD_API_THETAS:
+        out[theta] = [take("<f8") for _ in range(3)]
+    assert pos == len(data)
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("recipe,n", [("plummer", 20000), ("blobs", 12000), ("plummer", 1)])
+def test_build_api_transcription_matches_oracle(tmp_path, nbb_mod, oracle, recipe, n):
+    """The reference accuracy harness's call sequence, compiled against
+    nbb_build.hpp and run on the GPU: every intermediate and the
+    accelerations of each theta equal the oracle's bit for bit."""
+    import numpy as np
+    from nbb import ics
+
+    exe = str(tmp_path / "build_api_test")
+    _compile(os.path.join(ROOT, "tests", "cpp", "build_api_test.cpp"), exe,
+             [f"-L{PKG}", "-lnbb", f"-Wl,-rpath,{PKG}"])
+    p = ics.plummer(max(n, 2), seed=8) if recipe == "plummer" else ics.blobs(n, seed=9)
+    arrays = [np.ascontiguousarray(a[:n], dtype=np.float64) for a in (p.mass, p.x, p.y, p.z)]
+    src = tmp_path / "in.bin"
+    with open(src, "wb") as f:
+        f.write(struct.pack("<Q", n))
+        for a in arrays:
+            f.write(a.tobytes())
+    dst = tmp_path / "out.bin"
+    r = subprocess.run([exe, str(src), str(dst)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "ok"
+    got = _read_build_api_output(dst)
+    for theta in BUILD_API_THETAS:
+        ref = oracle.pipeline(*arrays, theta=theta, soft=0.02, g=1.0)
+        if theta == BUILD_API_THETAS[0]:
+            assert np.array_equal(got["box"], np.asarray(ref["box"]))
+            for f in BUILD_API_FIELDS[1:]:
+                assert np.array_equal(got[f], ref[f]), f
+        for a, b in zip(got[theta], (ref["ax"], ref["ay"], ref["az"])):
+            assert np.array_equal(a, b), theta
