@@ -343,11 +343,16 @@ int nbb_measure_fma_tflops(int precision, double *tflops);
  * pool or budget and forbids libraries to call cudaMalloc/cudaFree.  This call
  * allocates nothing: its scratch is one file-scope device array sized for
  * NBB_NOALLOC_MAX_PARTICLES particles (about 4.3 MB), held by every GPU that
- * loads the library until the process exits.  x, y, z, keys and idx are
- * device pointers of n elements; larger n is rejected with
+ * loads the library's device code until the process exits (with lazy module
+ * loading, CUDA's default, it is placed when the module loads, at the first
+ * call of the library on that device).  x, y, z, keys and idx are device
+ * pointers of n elements; larger n is rejected with
  * NBB_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress) and should come before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU (other
+ * capture; the address is kept per device number, so after a
+ * cudaDeviceReset, or from another context on the same device, the process
+ * must not call this entry point again.  Every call shares the array: calls
+ * that overlap on the GPU (other
  * streams, other threads) race and give wrong results.  The call synchronises
  * the given stream before it returns.  Its errors are reported by
  * nbb_noalloc_last_error_message(). */

@@ -68,3 +68,54 @@ def test_noalloc_sort_rejects_oversized_input(nbb_mod):
             C.c_void_p(out.data_ptr()), C.c_void_p(out.data_ptr()), None)
     assert st == 1  # NBB_ERR_INVALID_ARGUMENT
     assert "NBB_NOALLOC_MAX_PARTICLES" in msg().decode()
+
+
+def _raw_call(nbb_mod, x, y, z, keys, idx):
+    fn, msg = _bind(nbb_mod.load())
+    st = fn(C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), C.c_void_p(z.data_ptr()), x.numel(),
+            C.c_void_p(keys.data_ptr()), C.c_void_p(idx.data_ptr()), None)
+    return st, msg().decode()
+
+
+def test_noalloc_sort_reports_non_finite_input_then_recovers(nbb_mod):
+    # a NaN position is the reference's domain error; the error word in the
+    # shared scratch is cleared again by the next call
+    import torch
+    from nbb import ics
+
+    p = ics.plummer(5000, seed=11)
+    dev = torch.device("cuda:0")
+    x, y, z = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (p.x, p.y, p.z))
+    keys = torch.empty(5000, dtype=torch.int32, device=dev)
+    idx = torch.empty(5000, dtype=torch.int32, device=dev)
+    bad = x.clone()
+    bad[1234] = float("nan")
+    st, text = _raw_call(nbb_mod, bad, y, z, keys, idx)
+    assert st == 2 and "must be finite" in text  # NBB_ERR_DOMAIN
+    st, text = _raw_call(nbb_mod, x, y, z, keys, idx)
+    assert st == 0, text
+    _, _, _, ex = nbb_mod.compute_accelerations(p, 0.5, 0.01, 1.0, export=True)
+    assert np.array_equal(keys.cpu().numpy().view(np.uint32), ex["keys"])
+    assert np.array_equal(idx.cpu().numpy().view(np.uint32), ex["idx"])
+
+
+def test_noalloc_sort_takes_no_device_memory(nbb_mod):
+    # free device memory is unchanged across a call (the first call of the
+    # process may load the library's device module, so measure a later one)
+    import torch
+    from nbb import ics
+
+    p = ics.plummer(200_000, seed=12)
+    dev = torch.device("cuda:0")
+    x, y, z = (torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in (p.x, p.y, p.z))
+    keys = torch.empty(x.numel(), dtype=torch.int32, device=dev)
+    idx = torch.empty(x.numel(), dtype=torch.int32, device=dev)
+    st, text = _raw_call(nbb_mod, x, y, z, keys, idx)
+    assert st == 0, text
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(dev)
+    st, text = _raw_call(nbb_mod, x, y, z, keys, idx)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert st == 0, text
+    assert free1 == free0
