@@ -408,21 +408,36 @@ __global__ void __launch_bounds__(kSortThreads)
       st_release_u32(my, kDigitFlagP | run);
     } else {
       st_release_u32(my, kDigitFlagA | run);
+      // look back kLookback predecessors per round trip: their words are
+      // read together and summed in order up to the first inclusive prefix;
+      // a predecessor that has not published yet is read again (bounded)
+      constexpr int kLookback = 8;
       int j = tile - 1;
       int spins = 0;
-      while (j >= 0) {
-        const uint32_t st = ld_acquire_u32(status + (size_t)j * 256 + tid);
-        const uint32_t flag = st & ~kDigitMask;
-        if (flag == 0u) {
-          if (++spins > kSpinLimit) {
-            record_error(sc, kStageSort, kCodeTimeout);
-            break;
+      bool done = false;
+      while (!done) {
+        uint32_t w[kLookback];
+#pragma unroll
+        for (int k = 0; k < kLookback; ++k)
+          w[k] = (j - k >= 0) ? ld_acquire_u32(status + (size_t)(j - k) * 256 + tid) : kDigitFlagP;
+        int used = kLookback;
+#pragma unroll
+        for (int k = 0; k < kLookback; ++k) {
+          if (used < kLookback || done) continue;
+          const uint32_t flag = w[k] & ~kDigitMask;
+          if (flag == 0u) {
+            used = k;  // not published: resume here
+          } else {
+            prefix += w[k] & kDigitMask;
+            if (flag == kDigitFlagP) done = true;
           }
-          continue;
         }
-        prefix += st & kDigitMask;
-        if (flag == kDigitFlagP) break;
-        --j;
+        if (done) break;
+        j -= used;
+        if (used < kLookback && ++spins > kSpinLimit) {
+          record_error(sc, kStageSort, kCodeTimeout);
+          break;
+        }
       }
       st_release_u32(my, kDigitFlagP | (prefix + run));
     }
@@ -1247,6 +1262,15 @@ __global__ void __launch_bounds__(kBlock) layout_kernel(Workspace ws, double the
       kids[j++] = pre + ws.preoff[c];
     }
     ws.node_meta[pre] = make_int4(pre + size, pc > 0 ? f : -1, pc > 0 ? pc : 0, j);
+    if (ws.node_m) {
+      MixedNode rec;
+      rec.a = make_double4(comx, comy, comz, mass);
+      rec.cr2 = __double2float_ru(cm * cm * (1.0 + 0x1p-18));
+      rec.first = pc > 0 ? f : -1;
+      rec.count = pc > 0 ? pc : 0;
+      rec.nchild = j;
+      ws.node_m[pre] = rec;
+    }
     for (; j < 8; ++j) kids[j] = -1;
   }
 }

@@ -220,6 +220,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.mass, C); GET(ws.comx, C); GET(ws.comy, C); GET(ws.comz, C);
   GET(ws.node_a, C); GET(ws.node_b, C); GET(ws.node_c, C); GET(ws.node_meta, C);
   GET(ws.node_kids, 8 * C);
+  GET(ws.node_m, C);
 #undef GET
   e = cudaMemset(ws.sc, 0, sizeof(DevScalars));
   if (e != cudaSuccess) return e;

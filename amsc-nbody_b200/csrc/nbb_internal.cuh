@@ -83,6 +83,18 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
+// The mixed walk's record of one node (48 bytes, two 32-byte sectors):
+// centre of mass and mass, the squared acceptance radius for a target box
+// rounded up to FP32, and the node's particle range and child count.
+struct __align__(16) MixedNode {
+  double4 a;   // com x, y, z, mass
+  float cr2;   // (max(crit, sqrt(3) h + |com - centre|) (1 + 2^-40))^2 (1 + 2^-18), rounded up
+  int first;   // first particle of an occupied leaf, -1 otherwise
+  int count;   // particles of an occupied leaf, 0 otherwise
+  int nchild;  // children
+};
+static_assert(sizeof(MixedNode) == 48, "two 32-byte sectors per node");
+
 // Everything a spatial rebuild and a traversal touch, sized for capacity n.
 struct Workspace {
   int n = 0;            // particle count
@@ -166,6 +178,7 @@ struct Workspace {
   double4 *node_c = nullptr;  // crit, crit^2 lower/upper band, mixed walk's squared box radius
   int4 *node_meta = nullptr;  // skip, first particle, particle count, nchild
   int *node_kids = nullptr;   // 8 per node, preorder ids in visit order
+  MixedNode *node_m = nullptr;  // the mixed walk's records, preorder
   int *walk_ext = nullptr;    // walk_warps x walk_ext_cap: the mixed walk's stack below shared memory
 };
 

@@ -208,6 +208,7 @@ struct PairList {
 template <bool kTrackSource>
 struct MixedShared {
   double gbox[kMixedWarps][9];  // group box lo (3), hi (3), centre (3)
+  float ghalf[kMixedWarps][4];  // group box half extents, rounded up to FP32
   int stack[kMixedWarps][kStackCap];
   float4 la[kMixedWarps][kListCap / 2];
   float4 lb[kMixedWarps][kListCap / 2];
@@ -256,7 +257,7 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
   float2 px[kTPL], py[kTPL], pz[kTPL];
 #pragma unroll
   for (int q = 0; q < kTPL; ++q) px[q] = py[q] = pz[q] = make_float2(0.f, 0.f);
-  const float2 neg_half = make_float2(-0.5f, -0.5f), three_halves = make_float2(1.5f, 1.5f);
+  const float2 minus_three_halves = make_float2(-1.5f, -1.5f), five_halves = make_float2(2.5f, 2.5f);
   bool singular = false;
   const int pairs = (count + 1) >> 1;
 #pragma unroll kUnroll
@@ -268,9 +269,12 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
     for (int q = 0; q < kTPL; ++q) {
       const float2 dx = __fadd2_rn(ex, ntx[q]), dy = __fadd2_rn(ey, nty[q]), dz = __fadd2_rn(ez, ntz[q]);
       const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
-      float2 r = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-      r = __fmul2_rn(r, __ffma2_rn(__fmul2_rn(neg_half, r2), __fmul2_rn(r, r), three_halves));
-      float2 f = __fmul2_rn(em, __fmul2_rn(__fmul2_rn(r, r), r));
+      const float2 r = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+      // one Newton step for z = r2^(-3/2) from z0 = r^3 (Newton's method on
+      // z^(-2/3) - r2 = 0): z = z0 (5/2 - 3/2 r2 r^2)
+      const float2 rr = __fmul2_rn(r, r);
+      const float2 c = __ffma2_rn(__fmul2_rn(r2, rr), minus_three_halves, five_halves);
+      float2 f = __fmul2_rn(__fmul2_rn(em, c), __fmul2_rn(rr, r));
       if (kTrackSource) {
         const bool o0 = src[2 * pr] != self[q], o1 = src[2 * pr + 1] != self[q];
         singular |= (o0 && !(r2.x > 0.f) && em.x != 0.f) || (o1 && !(r2.y > 0.f) && em.y != 0.f);
@@ -368,19 +372,40 @@ __device__ __forceinline__ int warp_prefix_small(int v, unsigned lt, int &total)
   return excl;
 }
 
+// The group-box acceptance test of the mixed walk, in FP32.  The node's
+// centre of mass is taken relative to the group centre in FP64 and rounded
+// (the list entry's offset, returned in e); the squared distance from the
+// box (half extents rounded up) to that point is computed in FP32 and shrunk
+// by 2^-20 so that it never exceeds the exact FP64 distance, and cr2 is the
+// exact squared radius rounded up with a 2^-18 margin.  An accepted node is
+// therefore accepted by the exact test for every target in the box; a node
+// within the margins is opened instead (more work, never less accuracy).
+__device__ __forceinline__ bool accept_box(const double4 &a, const double *gbox, const float *ghalf, float cr2,
+                                           float4 &e) {
+  const float ox = (float)(a.x - gbox[6]), oy = (float)(a.y - gbox[7]), oz = (float)(a.z - gbox[8]);
+  constexpr float kShrink = 1.0f - 0x1p-20f;
+  const float ex = fmaxf(0.f, fmaf(fabsf(ox), kShrink, -ghalf[0]));
+  const float ey = fmaxf(0.f, fmaf(fabsf(oy), kShrink, -ghalf[1]));
+  const float ez = fmaxf(0.f, fmaf(fabsf(oz), kShrink, -ghalf[2]));
+  const float d2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex)) * kShrink;
+  e = make_float4(ox, oy, oz, (float)a.w);
+  return d2 > cr2;
+}
+
 // Mixed-precision traversal, one warp per target group of at most 32 x kTPL
 // Morton-consecutive targets inside one parent cell (kTPL targets per lane).
 // The group's bounding box (FP64) replaces the target in the reference's
 // acceptance test: a node is accepted for the whole group when the
 // box-to-centre-of-mass distance exceeds max(crit, sqrt(3) h + |com -
-// centre|) (crit = side/theta + |com - centre|, h the cell's half side;
-// node_c.w holds the square).  Every target in the box is then farther than
-// crit from the centre of mass and outside the cell, so the reference's test
-// accepts the node for each of them.  Nodes are examined 64 at a time (two per lane) from a
-// warp-private stack in shared memory, each lane fetching both nodes'
-// records and child lists in one round trip; a full stack spills its bottom
-// half to a global extension sized for any walk, so every node gets the
-// acceptance test.  Accepted nodes and the particles of reached leaves go to
+// centre|) (crit = side/theta + |com - centre|, h the cell's half side),
+// tested conservatively in FP32 (accept_box).  Every target in the box is
+// then farther than crit from the centre of mass and outside the cell, so
+// the reference's test accepts the node for each of them.  Nodes are
+// examined 64 at a time (two per lane) from a warp-private stack in shared
+// memory, each lane fetching both nodes' 48-byte records (MixedNode) in one
+// round trip and the child lists of the nodes that open; a full stack spills
+// its bottom half to a global extension sized for any walk, so every node
+// gets the acceptance test.  Accepted nodes and the particles of reached leaves go to
 // a shared interaction list as FP32 offsets from the group centre (formed in
 // FP64, then rounded) and are evaluated by all lanes in batches of 32.
 template <bool kTrackSource, int kTPL>
@@ -447,6 +472,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
           gb[a] = lo[a];
           gb[3 + a] = hi[a];
           gb[6 + a] = 0.5 * (lo[a] + hi[a]);
+          sh.ghalf[wid][a] = __double2float_ru(0.5 * (hi[a] - lo[a]));
         }
       }
       __syncwarp();
@@ -519,22 +545,20 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       int4 m0 = make_int4(0, 0, 0, 0), m1 = m0;
       int4 k00 = make_int4(-1, -1, -1, -1), k01 = k00, k10 = k00, k11 = k00;
       double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
-      double cr0 = 0.0, cr1 = 0.0;  // squared acceptance radius for a target box
+      float cr0 = 0.f, cr1 = 0.f;  // squared acceptance radius for a target box
       if (n0 >= 0) {
-        m0 = ws.node_meta[n0];
-        a0 = ws.node_a[n0];
-        cr0 = ws.node_c[n0].w;
-        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
-        k00 = kids[0];
-        k01 = kids[1];
+        const MixedNode &rec = ws.node_m[n0];
+        a0 = rec.a;
+        const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
+        cr0 = __int_as_float(meta.x);
+        m0 = make_int4(0, meta.y, meta.z, meta.w);
       }
       if (n1 >= 0) {
-        m1 = ws.node_meta[n1];
-        a1 = ws.node_a[n1];
-        cr1 = ws.node_c[n1].w;
-        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
-        k10 = kids[0];
-        k11 = kids[1];
+        const MixedNode &rec = ws.node_m[n1];
+        a1 = rec.a;
+        const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
+        cr1 = __int_as_float(meta.x);
+        m1 = make_int4(0, meta.y, meta.z, meta.w);
       }
       // 0 nothing, 1 accepted cell, 2 leaf, 3 open; the cell's list entry
       // (centre of mass offset from the group centre, mass) in FP32
@@ -546,17 +570,8 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
           if (m0.z > 0) {
             cat0 = 2;
           } else if (a.w != 0.0) {
-            // squared distance from the group box to the centre of mass
-            const double com[3] = {a.x, a.y, a.z};
-            double d2 = 0.0;
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-              const double e = fmax(0.0, fmax(gbox[ax] - com[ax], com[ax] - gbox[3 + ax]));
-              d2 = fma(e, e, d2);
-            }
             ++tests;
-            cat0 = (d2 > cr0) ? 1 : 3;
-            e0 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
+            cat0 = accept_box(a, gbox, sh.ghalf[wid], cr0, e0) ? 1 : 3;
           }
         }
       }
@@ -566,17 +581,8 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
           if (m1.z > 0) {
             cat1 = 2;
           } else if (a.w != 0.0) {
-            // squared distance from the group box to the centre of mass
-            const double com[3] = {a.x, a.y, a.z};
-            double d2 = 0.0;
-#pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-              const double e = fmax(0.0, fmax(gbox[ax] - com[ax], com[ax] - gbox[3 + ax]));
-              d2 = fma(e, e, d2);
-            }
             ++tests;
-            cat1 = (d2 > cr1) ? 1 : 3;
-            e1 = make_float4((float)(a.x - gbox[6]), (float)(a.y - gbox[7]), (float)(a.z - gbox[8]), (float)a.w);
+            cat1 = accept_box(a, gbox, sh.ghalf[wid], cr1, e1) ? 1 : 3;
           }
         }
       }
@@ -584,6 +590,18 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       // that would end past the stack accepts the node instead
       int nc0 = (cat0 == 3) ? min(max(m0.w, 0), 8) : 0;
       int nc1 = (cat1 == 3) ? min(max(m1.w, 0), 8) : 0;
+      // child lists only of the nodes that open; their loads overlap the
+      // prefix sums below
+      if (nc0 > 0) {
+        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
+        k00 = kids[0];
+        if (nc0 > 4) k01 = kids[1];
+      }
+      if (nc1 > 0) {
+        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
+        k10 = kids[0];
+        if (nc1 > 4) k11 = kids[1];
+      }
       int all_children;
       const int excl = warp_prefix_small<5>(nc0 + nc1, lt, all_children);
       int pushed = all_children;
