@@ -18,7 +18,8 @@
 //   level_bin_kernel      octree nodes binned by level
 //   propagate_level_kernel octree_physics.cu:156-245 (+ subtree sizes), one
 //                         level per launch, deepest first
-//   pre_level_kernel      preorder indices, one level per launch, root first
+//   ends_hist_kernel, ends_scan_kernel, preorder_kernel
+//                         preorder indices in closed form
 //   layout_kernel         traversal records in depth-first preorder
 //
 // No kernel synchronises with the host: data-dependent sizes (G, M) live in
@@ -68,7 +69,7 @@ __global__ void reset_scalars_kernel(DevScalars *sc) {
     sc->n_nodes = 0;
     sc->ticket_bbox = 0;
     sc->ticket_encode = 0;
-    for (int k = 0; k < 8; ++k) sc->tile_counter[k] = 0;
+    for (int k = 0; k < kTileCounters; ++k) sc->tile_counter[k] = 0;
     sc->work_counter = 0;
     sc->n_tgroups = 0;
     sc->stack_overflow = 0;
@@ -1186,27 +1187,71 @@ __global__ void __launch_bounds__(kBlock) propagate_level_kernel(Workspace ws, i
 // (barnes_hut.cu:283-293) is precomputed once per node, with a +-2^-44 band
 // around crit^2 inside which the traversal falls back to the exact
 // sqrt(d^2) > crit comparison.
-__global__ void __launch_bounds__(kBlock) pre_level_kernel(Workspace ws, int level) {
+// Preorder indices in closed form.  In a depth-first preorder that visits
+// children in octant order 7 -> 0 (descending Morton order), the nodes before
+// n are its ancestors and the nodes lying wholly after n in Morton order, so
+// with M nodes, size(n) the nodes of n's subtree and before(n) the nodes
+// lying wholly before it (their particle range ends before n's first
+// particle), pre(n) = M - size(n) - before(n).  before() is a count of range
+// ends per sorted particle index, scanned: two passes over the particles
+// instead of one launch per octree level.
+__global__ void __launch_bounds__(kBlock) ends_hist_kernel(Workspace ws) {
   DevScalars *sc = ws.sc;
-  const LevelScalars ls = level_scalars(ws, level);
-  const int m = ls.m, count = ls.count;
-  const int base = level_base(ws, level);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    const int node = ws.by_level[base + i];
-    if (node < 0 || node >= m) continue;
-    // the parent sits at a smaller level and got its index in an earlier launch
-    int pre = 0;
-    if (node != 0) {
-      const int par = ws.oparent[node];
-      if (par < 0 || par >= m || ws.olevel[par] >= level) {
-        record_error(sc, kStageLayout, 1);
-        continue;
-      }
-      pre = ws.pre_of[par] + ws.preoff[node];
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    const int last = ws.pfirst[node] + ws.psub[node] - 1;
+    if (ws.psub[node] < 1 || ws.pfirst[node] < 0 || last >= ws.n) {
+      record_error(sc, kStageLayout, 1);
+      continue;
     }
+    atomicAdd(&ws.pends[last], 1);
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) ends_scan_kernel(Workspace ws) {
+  __shared__ unsigned long long row_warp[kScanItems * (kScanThreads / 32)];
+  __shared__ unsigned long long s_total, s_prefix;
+  __shared__ int s_tile;
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int n = ws.n;
+  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&sc->tile_counter[kTileEnds], 1u);
+  __syncthreads();
+  const int tile = s_tile;
+  const int base = tile * kScanTile;
+  if (base >= n) return;
+  int val[kScanItems], excl[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    val[k] = (i < n) ? ws.pends[i] : 0;
+  }
+  const unsigned long long total = block_scan_rows<kScanItems, kScanThreads>(val, excl, row_warp, &s_total);
+  if (threadIdx.x < 32) {
+    const unsigned long long p =
+        warp_lookback(ws.scan_status + 2 * ws.scan_tiles_n + ws.scan_tiles_r, tile, total, sc, kStageLayout);
+    if (threadIdx.x == 0) s_prefix = p;
+  }
+  __syncthreads();
+  const int prefix = (int)s_prefix;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int i = base + k * kScanThreads + threadIdx.x;
+    if (i < n) ws.pends[i] = prefix + excl[k];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) preorder_kernel(Workspace ws) {
+  DevScalars *sc = ws.sc;
+  if (sc->error) return;
+  const int m = sc->n_nodes;
+  for (int node = blockIdx.x * blockDim.x + threadIdx.x; node < m; node += gridDim.x * blockDim.x) {
+    const int f = ws.pfirst[node];
+    const int pre = (f >= 0 && f < ws.n) ? m - ws.subtree[node] - ws.pends[f] : -1;
     if (pre < 0 || pre >= m) {
       record_error(sc, kStageLayout, 1);
-      pre = 0;
+      continue;
     }
     ws.pre_of[node] = pre;
   }
@@ -1461,7 +1506,7 @@ cudaError_t launch_step_reset(Workspace &ws, cudaStream_t s) {
   e = cudaMemsetAsync(ws.sort_status, 0, sizeof(uint32_t) * (size_t)ws.sort_passes * ws.sort_tiles * 256, s);
   if (e != cudaSuccess) return e;
   e = cudaMemsetAsync(ws.scan_status, 0,
-                      sizeof(unsigned long long) * (size_t)(2 * ws.scan_tiles_n + ws.scan_tiles_r), s);
+                      sizeof(unsigned long long) * (size_t)(3 * ws.scan_tiles_n + ws.scan_tiles_r), s);
   if (e != cudaSuccess) return e;
   if (ws.tflag) {
     e = cudaMemsetAsync(ws.tflag, 0, (size_t)ws.n, s);
@@ -1518,12 +1563,15 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   level_bin_kernel<<<grid, kBlock, 0, s>>>(ws);
   for (int level = ws.max_level; level >= 0; --level)
     propagate_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
-  for (int level = 0; level <= ws.max_level; ++level)
-    pre_level_kernel<<<level_grid(ws, level), kBlock, 0, s>>>(ws, level);
+  cudaError_t e = cudaMemsetAsync(ws.pends, 0, sizeof(int) * (size_t)ws.n, s);
+  if (e != cudaSuccess) return e;
+  ends_hist_kernel<<<grid, kBlock, 0, s>>>(ws);
+  ends_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  preorder_kernel<<<grid, kBlock, 0, s>>>(ws);
   layout_kernel<<<grid, kBlock, 0, s>>>(ws, theta);
   group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(9 + 2 * (ws.max_level + 1));
+  count_launches(12 + (ws.max_level + 1));
   return cudaGetLastError();
 }
 

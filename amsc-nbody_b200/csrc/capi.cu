@@ -205,7 +205,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.sort_status, (size_t)ws.sort_passes * ws.sort_tiles * 256);
   ws.scan_tiles_n = (n + kScanTile - 1) / kScanTile;
   ws.scan_tiles_r = (2 * n - 1 + kScanTile - 1) / kScanTile;
-  GET(ws.scan_status, (size_t)(2 * ws.scan_tiles_n + ws.scan_tiles_r));
+  GET(ws.scan_status, (size_t)(3 * ws.scan_tiles_n + ws.scan_tiles_r));
   GET(ws.keys, N); GET(ws.idx, N); GET(ws.pm4, N); GET(ws.psys, N);
   GET(ws.ukey, N); GET(ws.uniq, N); GET(ws.gfirst, N); GET(ws.gcount, N); GET(ws.glast, N);
   GET(ws.left, N); GET(ws.right, N); GET(ws.rfirst, N); GET(ws.rlast, N); GET(ws.plen, N);
@@ -214,7 +214,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.children, 8 * C);
   GET(ws.oparent, C); GET(ws.olevel, C); GET(ws.oprefix, C); GET(ws.ofirst, C); GET(ws.ocount, C);
   GET(ws.child_count, C); GET(ws.pre_of, C); GET(ws.by_level, C); GET(ws.subtree, C); GET(ws.preoff, C);
-  GET(ws.psub, C); GET(ws.pfirst, C);
+  GET(ws.psub, C); GET(ws.pfirst, C); GET(ws.pends, N);
   GET(ws.tflag, N); GET(ws.tstart, N);
   GET(ws.cx, C); GET(ws.cy, C); GET(ws.cz, C); GET(ws.half, C);
   GET(ws.mass, C); GET(ws.comx, C); GET(ws.comy, C); GET(ws.comz, C);

@@ -43,7 +43,7 @@ struct DevScalars {
   int error;                     // sticky first error (not reset per step)
   unsigned int ticket_bbox;
   unsigned int ticket_encode;
-  unsigned int tile_counter[8];  // dynamic tile ids: sort passes, then scans
+  unsigned int tile_counter[9];  // dynamic tile ids: sort passes, then scans
   unsigned int work_counter;     // traversal work queue
   int n_tgroups;                 // traversal target groups
   unsigned int stack_overflow;   // mixed traversal nodes accepted on overflow
@@ -77,6 +77,8 @@ constexpr int kMaxSystems = 512;
 constexpr int kTileGroups = kMaxSortPasses;      // 5
 constexpr int kTilePlan = kMaxSortPasses + 1;    // 6
 constexpr int kTileTargetGroups = kMaxSortPasses + 2;  // 7
+constexpr int kTileEnds = kMaxSortPasses + 3;          // 8
+constexpr int kTileCounters = kMaxSortPasses + 4;      // 9
 
 // Single-pass scan tiling.
 constexpr int kScanThreads = 256;
@@ -166,6 +168,7 @@ struct Workspace {
   double *mass = nullptr, *comx = nullptr, *comy = nullptr, *comz = nullptr;
   int *subtree = nullptr, *preoff = nullptr;
   int *psub = nullptr, *pfirst = nullptr;  // particles in a subtree / its first
+  int *pends = nullptr;   // n: octree nodes whose particle range ends at each sorted index, then their exclusive scan
 
   // traversal target groups: contiguous Morton ranges of <= kGroupMax
   // particles inside one parent cell
