@@ -409,36 +409,21 @@ __global__ void __launch_bounds__(kSortThreads)
       st_release_u32(my, kDigitFlagP | run);
     } else {
       st_release_u32(my, kDigitFlagA | run);
-      // look back kLookback predecessors per round trip: their words are
-      // read together and summed in order up to the first inclusive prefix;
-      // a predecessor that has not published yet is read again (bounded)
-      constexpr int kLookback = 8;
       int j = tile - 1;
       int spins = 0;
-      bool done = false;
-      while (!done) {
-        uint32_t w[kLookback];
-#pragma unroll
-        for (int k = 0; k < kLookback; ++k)
-          w[k] = (j - k >= 0) ? ld_acquire_u32(status + (size_t)(j - k) * 256 + tid) : kDigitFlagP;
-        int used = kLookback;
-#pragma unroll
-        for (int k = 0; k < kLookback; ++k) {
-          if (used < kLookback || done) continue;
-          const uint32_t flag = w[k] & ~kDigitMask;
-          if (flag == 0u) {
-            used = k;  // not published: resume here
-          } else {
-            prefix += w[k] & kDigitMask;
-            if (flag == kDigitFlagP) done = true;
+      while (j >= 0) {
+        const uint32_t st = ld_acquire_u32(status + (size_t)j * 256 + tid);
+        const uint32_t flag = st & ~kDigitMask;
+        if (flag == 0u) {
+          if (++spins > kSpinLimit) {
+            record_error(sc, kStageSort, kCodeTimeout);
+            break;
           }
+          continue;
         }
-        if (done) break;
-        j -= used;
-        if (used < kLookback && ++spins > kSpinLimit) {
-          record_error(sc, kStageSort, kCodeTimeout);
-          break;
-        }
+        prefix += st & kDigitMask;
+        if (flag == kDigitFlagP) break;
+        --j;
       }
       st_release_u32(my, kDigitFlagP | (prefix + run));
     }

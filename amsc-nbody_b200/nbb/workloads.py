@@ -173,7 +173,7 @@ def _kind_mask(coords, kind):
     return np.array([w in names for w, _ in coords])
 
 
-def adjoint(n=65536, steps=1000, every=32, fd_coords=64, fd_chunk=16, n_direct=4096):
+def adjoint(n=65536, steps=1000, every=32, fd_coords=64, fd_chunk=16, n_direct=4096, h=1e-4, h_mass=0.1):
     torch = _torch()
     p = ics.plummer(n, seed=0)
     rng = np.random.Generator(np.random.Philox(4321))
@@ -220,7 +220,7 @@ def adjoint(n=65536, steps=1000, every=32, fd_coords=64, fd_chunk=16, n_direct=4
     target64 = grads["fp64"][3]
     fd = np.zeros(len(coords))
     fd_central = np.zeros(len(coords))
-    hs = np.array([1e-3 * float(p.mass[k]) if w == "mass" else 1e-6 for w, k in coords])
+    hs = np.array([h_mass * float(p.mass[k]) if w == "mass" else h for w, k in coords])
     t0 = time.perf_counter()
     for c0 in range(0, len(coords), fd_chunk):
         chunk = coords[c0:c0 + fd_chunk]
@@ -237,7 +237,7 @@ def adjoint(n=65536, steps=1000, every=32, fd_coords=64, fd_chunk=16, n_direct=4
                 d.append(np.sum((xp - xm) * (xp + xm - 2.0 * target64)) / n / (2.0 * h * (1 + j // 2)))
             fd_central[c0 + i] = d[0]
             fd[c0 + i] = (4.0 * d[0] - d[1]) / 3.0
-    fdinfo = {"coords": len(coords), "h_positions_velocities": 1e-6, "h_mass": "1e-3 * m",
+    fdinfo = {"coords": len(coords), "h_positions_velocities": h, "h_mass": f"{h_mass} * m",
               "richardson": "(4 D(h) - D(2h)) / 3", "seconds": time.perf_counter() - t0}
     per = {}
     for name in ("fp64", "mixed"):
