@@ -35,7 +35,6 @@
 #include "nbb_internal.cuh"
 #include "walk_fp64.cuh"
 
-#include <algorithm>
 #include <climits>
 #include <cmath>
 
@@ -132,33 +131,20 @@ __global__ void __launch_bounds__(kBlock) adj_topology_kernel(Workspace ws, int 
 // Vector-Jacobian product of the frozen-structure force: the plain walk's
 // node sequence per lane (same records, same acceptance test), with the
 // accelerations cotangent coef * gv of each target.
-//
-// A target group's walk is split into `pieces` work items over consecutive
-// ranges of the preorder (more warps when the groups alone would leave the
-// GPU partly idle).  The item of range [lo, hi) walks the same lane paths
-// but adds only the interactions of nodes inside its range: a node before lo
-// whose subtree ends by lo is skipped, one whose subtree reaches into the
-// range gets the acceptance test only (an accepted one ends the lane's walk
-// of that subtree, as it does in the whole walk), and the walk stops at hi.
-// Every interaction of the whole walk is thus taken exactly once; a target's
-// own cotangent is added atomically when the walk is split.
-__global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, TraversalParams p, AdjointBuffers ab,
-                                                           int pieces) {
+__global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, TraversalParams p, AdjointBuffers ab) {
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int lane = threadIdx.x & 31;
   const int n = ws.n;
   const int m = sc->n_nodes;
   const int n_groups = p.group_mode ? sc->n_tgroups : (n + 31) >> 5;
-  const long long n_items = (long long)n_groups * pieces;
   const double g = p.g;
   bool singular = false;
   while (true) {
-    int item = 0;
-    if (lane == 0) item = (int)atomicAdd(&sc->work_counter, 1u);
-    item = __shfl_sync(kFull, item, 0);
-    if (item >= n_items) break;
-    const int grp = item / pieces, piece = item % pieces;
+    int grp = 0;
+    if (lane == 0) grp = (int)atomicAdd(&sc->work_counter, 1u);
+    grp = __shfl_sync(kFull, grp, 0);
+    if (grp >= n_groups) break;
     const int g0 = p.group_mode ? ws.tstart[grp] : grp * 32;
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32, n);
     // a group larger than a warp is walked 32 targets at a time
@@ -178,30 +164,16 @@ __global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, Travers
       const int sys = ws.n_systems > 1 ? ws.psys[g0] : 0;
       const int root = ws.root_pre[sys];
       const int end = (root >= 0 && root < m) ? min(ws.node_meta[root].x, m) : 0;
-      const long long span = end > root ? end - root : 0;
-      const int lo = (int)(root + span * piece / pieces);
-      const int hi = (int)(root + span * (piece + 1) / pieces);
       const double soft = ws.sys_eps ? ws.sys_eps[sys] : p.soft;
       const double soft2 = __dmul_rn(soft, soft);
       double gtx = 0.0, gty = 0.0, gtz = 0.0;
       int resume = valid ? root : INT_MAX;
       int node = __reduce_min_sync(kFull, resume);
-      while (node < hi) {
+      while (node < end) {
         const int4 meta = ws.node_meta[node];
         const double4 a = ws.node_a[node];
         const bool here = resume == node;
-        if (node < lo) {
-          // before this item's range (warp-uniform): only the lane paths
-          if (here) {
-            if (meta.x <= lo || meta.z > 0 || a.w == 0.0) {
-              resume = meta.x;
-            } else {
-              double dx, dy, dz, d2;
-              const bool acc = accept_fp64(a, ws.node_b + node, ws.node_c[node], t, dx, dy, dz, d2);
-              resume = acc ? meta.x : node + 1;
-            }
-          }
-        } else if (meta.z > 0) {
+        if (meta.z > 0) {
           // two particles at a time: both products are formed (independent
           // square roots and divisions) before they are added and scattered
           // in particle order
@@ -274,16 +246,7 @@ __global__ void __launch_bounds__(256) adjoint_walk_kernel(Workspace ws, Travers
         if (resume <= node) resume = node + 1;
         node = __reduce_min_sync(kFull, resume);
       }
-      if (valid) {
-        if (pieces == 1) {
-          ab.tgt_g[s] = make_double4(gtx, gty, gtz, 0.0);
-        } else {
-          double *d = reinterpret_cast<double *>(ab.tgt_g + s);
-          atomicAdd(d + 0, gtx);
-          atomicAdd(d + 1, gty);
-          atomicAdd(d + 2, gtz);
-        }
-      }
+      if (valid) ab.tgt_g[s] = make_double4(gtx, gty, gtz, 0.0);
     }
   }
   if (__any_sync(kFull, singular) && lane == 0) record_error(sc, kStageTraversal, 6);
@@ -574,19 +537,10 @@ cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const 
   cudaError_t e = cudaMemsetAsync(ab.node_g, 0, sizeof(double4) * (size_t)ws.cap_nodes, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(ab.part_g, 0, sizeof(double4) * (size_t)ws.n, s);
   if (e != cudaSuccess) return e;
-  // walk pieces per target group: about 48 warps per SM in all (one-warp
-  // groups hold some 24 targets on average), at most 8 pieces
-  const long long groups_est = ws.n / 24 + 1;
-  const long long want = (long long)(ws.num_sms > 0 ? ws.num_sms : 148) * 48;
-  const int pieces = (int)std::min(8ll, std::max(1ll, (want + groups_est - 1) / groups_est));
-  if (pieces > 1) {
-    e = cudaMemsetAsync(ab.tgt_g, 0, sizeof(double4) * (size_t)ws.n, s);
-    if (e != cudaSuccess) return e;
-  }
   const int grid = grid_of_ws(ws, 8);
   adj_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
   adj_topology_kernel<<<grid, kBlock, 0, s>>>(ws, ab.pparent, ab.prange, nullptr);
-  adjoint_walk_kernel<<<grid_of_ws(ws, 8), 256, 0, s>>>(ws, p, ab, pieces);
+  adjoint_walk_kernel<<<grid_of_ws(ws, 8), 256, 0, s>>>(ws, p, ab);
   adj_node_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
   adj_leaf_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
   count_launches(5);

@@ -1145,7 +1145,11 @@ int nbb_accel_direct(size_t n, const double *mass, const double *x, const double
   double *oa[3] = {ax, ay, az};
   double *da[3] = {ax, ay, az};
   for (int k = 0; k < 3 && e == cudaSuccess && !on_device; ++k) e = al.get(da[k], (size_t)n_targets);
-  if (e == cudaSuccess) e = launch_direct(n, dm, dx, dy, dz, n_targets, dt, g, softening, da[0], da[1], da[2], s);
+  double *part = nullptr;
+  const int chunks = direct_chunks(n, n_targets);
+  if (e == cudaSuccess && chunks > 1) e = al.get(part, (size_t)chunks * 3 * n_targets);
+  if (e == cudaSuccess)
+    e = launch_direct(n, dm, dx, dy, dz, n_targets, dt, g, softening, da[0], da[1], da[2], part, s);
   for (int k = 0; k < 3 && e == cudaSuccess && !on_device; ++k)
     e = cudaMemcpyAsync(oa[k], da[k], (size_t)n_targets * sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1914,10 +1918,10 @@ int nbb_direct_rollout_adjoint(const nbb_config *cfg, size_t n, const double *ma
     return r;
   };
   e = store(0);
-  if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, s);
+  if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, nullptr, s);
   for (uint64_t t = 1; t <= steps && e == cudaSuccess; ++t) {
     e = launch_kick_drift(X, Y, Z, VX, VY, VZ, AX, AY, AZ, n, dt, s);
-    if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, s);
+    if (e == cudaSuccess) e = launch_direct(n, M, X, Y, Z, (int)n, nullptr, G, eps, AX, AY, AZ, nullptr, s);
     if (e == cudaSuccess) e = launch_kick(VX, VY, VZ, AX, AY, AZ, n, dt, s);
     if (e == cudaSuccess) e = store(t);
   }

@@ -292,10 +292,16 @@ cudaError_t launch_kick_drift(double *x, double *y, double *z, double *vx,
                               const double *ay, const double *az, size_t n,
                               double dt, cudaStream_t s);
 // FP64 direct sum for a target list.
+// Source chunks the direct sum uses for n sources and n_targets targets (1:
+// each target's sum in one pass in index order, bit for bit the sequential
+// sum; more: partial sums of consecutive source ranges added in range order,
+// for few targets over many sources).  part holds chunks * 3 * n_targets.
+int direct_chunks(size_t n, int n_targets);
 cudaError_t launch_direct(size_t n, const double *m, const double *x,
                           const double *y, const double *z, int n_targets,
                           const int *targets, double g, double soft,
-                          double *ax, double *ay, double *az, cudaStream_t s);
+                          double *ax, double *ay, double *az, double *part,
+                          cudaStream_t s);
 // Traversal on a caller octree in the reference numbering (FP64 plain).
 struct RefOctree {
   int n_nodes, n_particles;

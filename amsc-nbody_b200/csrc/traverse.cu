@@ -772,24 +772,31 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
 constexpr int kDirectThreads = 128;
 
 // barnes_hut_accuracy_test.cu:101-172: each thread sums every other particle
-// in index order; sources are staged through shared memory in tiles.
+// in index order; sources are staged through shared memory in tiles.  With
+// chunked sources (blockIdx.y of gridDim.y chunks, partial sums to
+// part[chunk][3][n_targets]) few targets still fill the GPU; the partials are
+// then added in chunk order by direct_combine_kernel.
 __global__ void __launch_bounds__(kDirectThreads)
     direct_kernel(int n, const double *__restrict__ m, const double *__restrict__ x,
                   const double *__restrict__ y, const double *__restrict__ z, int n_targets,
                   const int *__restrict__ targets, double g, double soft2, double *ax, double *ay,
-                  double *az) {
+                  double *az, double *part) {
   __shared__ double4 tile[kDirectThreads];
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int chunks = gridDim.y;
+  const long long span = ((long long)n + chunks - 1) / chunks;
+  const int j0 = (int)min((long long)n, span * blockIdx.y);
+  const int j1 = (int)min((long long)n, span * (blockIdx.y + 1));
   int t = (k < n_targets) ? (targets ? targets[k] : k) : 0;
   const bool active = k < n_targets && t >= 0 && t < n;
   if (!active) t = 0;
   const double tx = active ? x[t] : 0.0, ty = active ? y[t] : 0.0, tz = active ? z[t] : 0.0;
   double rx = 0.0, ry = 0.0, rz = 0.0;
-  for (int base = 0; base < n; base += kDirectThreads) {
+  for (int base = j0; base < j1; base += kDirectThreads) {
     const int j = base + threadIdx.x;
-    tile[threadIdx.x] = (j < n) ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
+    tile[threadIdx.x] = (j < j1) ? make_double4(x[j], y[j], z[j], m[j]) : make_double4(0, 0, 0, 0);
     __syncthreads();
-    const int lim = (n - base < kDirectThreads) ? n - base : kDirectThreads;
+    const int lim = (j1 - base < kDirectThreads) ? j1 - base : kDirectThreads;
     if (active) {
       for (int q = 0; q < lim; ++q) {
         if (base + q == t) continue;
@@ -806,10 +813,34 @@ __global__ void __launch_bounds__(kDirectThreads)
     __syncthreads();
   }
   if (k < n_targets) {
-    ax[k] = active ? rx : NAN;
-    ay[k] = active ? ry : NAN;
-    az[k] = active ? rz : NAN;
+    if (chunks == 1) {
+      ax[k] = active ? rx : NAN;
+      ay[k] = active ? ry : NAN;
+      az[k] = active ? rz : NAN;
+    } else {
+      double *pc = part + (size_t)blockIdx.y * 3 * n_targets;
+      pc[k] = active ? rx : NAN;
+      pc[n_targets + k] = active ? ry : NAN;
+      pc[2 * (size_t)n_targets + k] = active ? rz : NAN;
+    }
   }
+}
+
+__global__ void __launch_bounds__(kDirectThreads)
+    direct_combine_kernel(const double *__restrict__ part, int chunks, int n_targets, double *ax, double *ay,
+                          double *az) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n_targets) return;
+  double rx = 0.0, ry = 0.0, rz = 0.0;
+  for (int c = 0; c < chunks; ++c) {
+    const double *pc = part + (size_t)c * 3 * n_targets;
+    rx = __dadd_rn(rx, pc[k]);
+    ry = __dadd_rn(ry, pc[n_targets + k]);
+    rz = __dadd_rn(rz, pc[2 * (size_t)n_targets + k]);
+  }
+  ax[k] = rx;
+  ay[k] = ry;
+  az[k] = rz;
 }
 
 // ------------------------------------------- reference-layout octree ----
@@ -1138,13 +1169,23 @@ cudaError_t launch_kick_drift(double *x, double *y, double *z, double *vx, doubl
   return cudaGetLastError();
 }
 
+int direct_chunks(size_t n, int n_targets) {
+  const int blocks = (n_targets + kDirectThreads - 1) / kDirectThreads;
+  const int want = device_sms() * 8;  // blocks that keep every SM busy
+  if (blocks >= want || n < 65536) return 1;
+  const long long c = std::min<long long>((want + blocks - 1) / blocks, (long long)(n / 4096));
+  return (int)std::max(1ll, std::min(c, 256ll));
+}
+
 cudaError_t launch_direct(size_t n, const double *m, const double *x, const double *y, const double *z,
                           int n_targets, const int *targets, double g, double soft, double *ax,
-                          double *ay, double *az, cudaStream_t s) {
-  const int blocks = (n_targets + kDirectThreads - 1) / kDirectThreads;
-  direct_kernel<<<blocks > 0 ? blocks : 1, kDirectThreads, 0, s>>>((int)n, m, x, y, z, n_targets, targets,
-                                                                  g, soft * soft, ax, ay, az);
-  count_launches(1);
+                          double *ay, double *az, double *part, cudaStream_t s) {
+  const int blocks = std::max(1, (n_targets + kDirectThreads - 1) / kDirectThreads);
+  const int chunks = part ? direct_chunks(n, n_targets) : 1;
+  direct_kernel<<<dim3(blocks, chunks), kDirectThreads, 0, s>>>((int)n, m, x, y, z, n_targets, targets, g,
+                                                                soft * soft, ax, ay, az, part);
+  if (chunks > 1) direct_combine_kernel<<<blocks, kDirectThreads, 0, s>>>(part, chunks, n_targets, ax, ay, az);
+  count_launches(chunks > 1 ? 2 : 1);
   return cudaGetLastError();
 }
 

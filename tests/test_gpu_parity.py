@@ -233,6 +233,18 @@ def test_direct_sum_matches_oracle(nbb_mod, oracle):
     assert np.array_equal(a, e)
 
 
+def test_direct_sum_over_source_chunks_matches_oracle(nbb_mod, oracle):
+    # few targets over many sources: partial sums of consecutive source
+    # ranges, added in range order -- the sequential sum up to rounding
+    from nbb import ics
+
+    p = ics.plummer(200_000, seed=14)
+    tg = np.sort(np.random.default_rng(3).choice(200_000, 1000, replace=False)).astype(np.int32)
+    a = np.stack(nbb_mod.compute_direct_accelerations(p.mass, p.x, p.y, p.z, 1.0, 0.01, targets=tg))
+    e = np.stack(oracle.direct_accel(p.mass, p.x, p.y, p.z, 1.0, 0.01, targets=tg))
+    assert rel_err(a, e) <= 1e-13
+
+
 # --------------------------------------------------- simulation API ---
 
 def test_simulation_trajectory_matches_oracle(nbb_mod, oracle):
