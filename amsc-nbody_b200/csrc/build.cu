@@ -1406,6 +1406,475 @@ __global__ void __launch_bounds__(kScanThreads) group_scan_kernel(Workspace ws) 
   if (base + kScanTile >= n && threadIdx.x == 0) sc->n_tgroups = prefix + (int)total;
 }
 
+// ------------------------------------------------- level-order build ----
+//
+// The step's octree, built from the sorted unique keys without the radix
+// tree.  The octree the reference derives from the Karras tree
+// (radix_to_octree.cu:70-145, octree_builder.cu:87-224) holds, for every leaf
+// group g of the G sorted unique keys u[0..G), the cells of u[g]'s prefixes
+// from the root down to level lambda_g = 1 + max(0, delta_g, delta_{g+1}),
+// where delta_g is the number of octree levels u[g-1] and u[g] share (-1 past
+// either end): a leaf sits one level below its radix parent, whose prefix is
+// the longer of the leaf's two common prefixes.  Group g is the first group
+// of its cells at levels (delta_g, lambda_g] and the last group of its cells
+// at levels (delta_{g+1}, lambda_g].
+//
+// Numbered level by level, each level in ascending key order, the children of
+// a cell (octants 0..7) are consecutive entries of the next level.  A
+// depth-first preorder that visits children octant 7 -> 0 meets the groups in
+// descending key order, group g adding its cells at levels (delta_{g+1},
+// lambda_g] top-down; with S(g) the number of cells added by the groups >= g,
+// the cell at level L whose last group is g has preorder index
+// S(g) - lambda_g + L - 1, and a cell's subtree ends at S(its first group).
+// One scan over the groups numbers every cell and gives its first child and
+// its preorder range; mass and centre of mass are then combined level by
+// level, deepest first, from the consecutive child records in octant order
+// (octree_physics.cu:156-245), and the traversal records are written at the
+// preorder index in the same pass.
+
+// Octree levels two distinct keys of key_bits bits share.
+__device__ __forceinline__ int common_levels(unsigned long long a, unsigned long long b, int key_bits) {
+  return (__clzll((long long)(a ^ b)) - (64 - key_bits)) / kDims;
+}
+
+// Per group: the level span (delta, lambda, delta of the next group) and the
+// particle count; per tile of kScanTile groups: the cells its groups start at
+// each level and the cells they end.
+__global__ void __launch_bounds__(kScanThreads) lo_span_kernel(Workspace ws) {
+  __shared__ int s_cnt[kLevelOrderChannels];
+  __shared__ int s_g;
+  constexpr int kEnded = kMaxLevels;  // channel of the ended cells
+  DevScalars *sc = ws.sc;
+  if (threadIdx.x == 0) {
+    const int g = sc->n_groups;
+    const bool ok = g > 0 && g <= ws.n;
+    if (!ok && blockIdx.x == 0) record_error(sc, kStageGroups, 2);
+    s_g = ok ? g : 0;
+  }
+  if (threadIdx.x < kLevelOrderChannels) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int G = s_g, kb = ws.key_bits;
+  const int base = blockIdx.x * kScanTile;
+#pragma unroll 1
+  for (int k = 0; k < kScanItems; ++k) {
+    const int g = base + k * kScanThreads + threadIdx.x;
+    if (g >= G) break;
+    ws.gcount[g] = ws.glast[g] - ws.gfirst[g] + 1;
+    const unsigned long long key = ws.ukey[g];
+    int d = -1, dn = -1;
+    bool bad = (key >> kb) != 0ull;
+    if (g > 0) {
+      const unsigned long long kp = ws.ukey[g - 1];
+      if (kp >= key) bad = true;
+      else d = common_levels(kp, key, kb);
+    }
+    if (g + 1 < G) {
+      const unsigned long long kn = ws.ukey[g + 1];
+      if (kn <= key) bad = true;
+      else dn = common_levels(key, kn, kb);
+    }
+    const int lam = 1 + max(0, max(d, dn));
+    if (bad || lam > ws.max_level) {
+      record_error(sc, kStagePlan, bad ? 1 : 3);
+      continue;
+    }
+    ws.gspan[g] = (d + 1) | (lam << 8) | ((dn + 1) << 16);
+    for (int l = d + 1; l <= lam; ++l) atomicAdd(&s_cnt[l], 1);
+    atomicAdd(&s_cnt[kEnded], lam - dn);
+  }
+  __syncthreads();
+  if (threadIdx.x < kLevelOrderChannels)
+    ws.lo_tiles[(size_t)blockIdx.x * kLevelOrderChannels + threadIdx.x] = s_cnt[threadIdx.x];
+}
+
+// Exclusive prefixes of the per-tile counts, one warp per channel, in place;
+// the totals give the cells per level and M (the node count).
+__global__ void __launch_bounds__(32 * kLevelOrderChannels) lo_tile_scan_kernel(Workspace ws) {
+  constexpr int kEnded = kMaxLevels;
+  __shared__ long long s_total[kLevelOrderChannels];
+  DevScalars *sc = ws.sc;
+  const int g = sc->n_groups;
+  const int G = (g > 0 && g <= ws.n) ? g : 0;
+  const int tiles = (G + kScanTile - 1) / kScanTile;
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long carry = 0;
+  for (int t0 = 0; t0 < tiles; t0 += 32) {
+    const int t = t0 + lane;
+    int *p = ws.lo_tiles + (size_t)t * kLevelOrderChannels + c;
+    const int v = (t < tiles) ? *p : 0;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += u;
+    }
+    if (t < tiles) *p = (int)(carry + inc - v);
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) s_total[c] = carry;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long m = 0;
+    for (int l = 0; l < kMaxLevels; ++l) {
+      sc->level_count[l] = (int)s_total[l];
+      m += s_total[l];
+    }
+    if (G == 0 || m != s_total[kEnded] || m > ws.cap_nodes) {
+      if (G > 0) record_error(sc, m > ws.cap_nodes ? kStagePlan : kStageLayout, m > ws.cap_nodes ? kCodeOverflow : 1);
+      sc->n_nodes = 0;
+    } else {
+      sc->n_nodes = (int)m;
+    }
+  }
+}
+
+// Cell numbers: per tile, the cells started by the groups before it (the
+// tile prefixes) plus the ranks inside the tile.  Writes each cell's first
+// group, first child and subtree end (by its first group) and its last group
+// and preorder index (by its last group).
+__global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
+  constexpr int kWarps = kScanThreads / 32;
+  constexpr int kNodes = kMaxLevels;  // channel of the ended cells (the node count S)
+  static_assert(kNodes < kLevelOrderChannels, "one warp holds every channel");
+  __shared__ int s_warp[kWarps][kLevelOrderChannels];
+  __shared__ int s_prefix[kLevelOrderChannels];
+  __shared__ int s_base[kMaxLevels + 2];
+  __shared__ int s_g, s_m;
+  DevScalars *sc = ws.sc;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tile = blockIdx.x;
+  if (tid == 0) {
+    const int g = sc->n_groups, m = sc->n_nodes;
+    s_g = (g > 0 && g <= ws.n && m > 0) ? g : 0;
+    s_m = m;
+    int run = 0;
+    for (int l = 0; l < kMaxLevels; ++l) {
+      s_base[l] = run;
+      run += sc->level_count[l];
+    }
+    s_base[kMaxLevels] = s_base[kMaxLevels + 1] = run;
+  }
+  if (tid < kLevelOrderChannels) s_prefix[tid] = ws.lo_tiles[(size_t)tile * kLevelOrderChannels + tid];
+  __syncthreads();
+  const int G = s_g, M = s_m;
+  const int base = tile * kScanTile;
+  if (G == 0 || base >= G) return;
+  const int max_level = ws.max_level;
+  // each warp owns 32 * kScanItems consecutive groups, item k at g0 + 32 k;
+  // a group's cells: started at levels (delta, lambda], ended at (delta_next, lambda]
+  const int g0 = base + warp * (32 * kScanItems) + lane;
+  auto masks = [&](int g, unsigned &smask, unsigned &lmask, int &lam) {
+    smask = lmask = 0u;
+    lam = 0;
+    if (g >= G) return;
+    const int sp = ws.gspan[g];
+    const int d = (sp & 255) - 1, l = (sp >> 8) & 255, dn = ((sp >> 16) & 255) - 1;
+    if (l < 1 || l > max_level || d >= l || dn >= l) {
+      record_error(sc, kStagePlan, 3);
+      return;
+    }
+    const unsigned upto = (2u << l) - 1u;  // levels 0..lambda
+    smask = upto & ~((1u << (d + 1)) - 1u);
+    lmask = upto & ~((1u << (dn + 1)) - 1u);
+    lam = l;
+  };
+  // this warp's cells per level (lane l) and node count (lane kNodes)
+  int cnt[kMaxLevels];
+#pragma unroll
+  for (int l = 0; l < kMaxLevels; ++l) cnt[l] = 0;
+  int e = 0;
+#pragma unroll 1
+  for (int k = 0; k < kScanItems; ++k) {
+    unsigned sm, lm;
+    int lam;
+    masks(g0 + 32 * k, sm, lm, lam);
+#pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) cnt[l] += (int)((sm >> l) & 1u);
+    e += __popc(lm);
+  }
+  int mine = __reduce_add_sync(0xffffffffu, e);
+  mine = (lane == kNodes) ? mine : 0;
+#pragma unroll
+  for (int l = 0; l < kMaxLevels; ++l) {
+    const int c = __reduce_add_sync(0xffffffffu, cnt[l]);
+    if (lane == l) mine = c;
+  }
+  s_warp[warp][lane] = mine;
+  __syncthreads();
+  if (warp == 0) {
+    // channel `lane`: the warps' exclusive offsets inside the tile
+    int tot = 0;
+    for (int w = 0; w < kWarps; ++w) {
+      const int v = s_warp[w][lane];
+      s_warp[w][lane] = tot;
+      tot += v;
+    }
+  }
+  __syncthreads();
+  const unsigned lt = lanemask_lt();
+  int run[kMaxLevels];
+#pragma unroll
+  for (int l = 0; l < kMaxLevels; ++l) run[l] = s_prefix[l] + s_warp[warp][l];
+  int nrun = s_prefix[kNodes] + s_warp[warp][kNodes];
+#pragma unroll 1
+  for (int k = 0; k < kScanItems; ++k) {
+    const int g = g0 + 32 * k;
+    unsigned sm, lm;
+    int lam;
+    masks(g, sm, lm, lam);
+    const int ek = __popc(lm);
+    int inc = ek;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const int s_from = M - (nrun + inc - ek);  // S(g): cells added by groups >= g
+    nrun += __shfl_sync(0xffffffffu, inc, 31);
+    int excl[kMaxLevels + 1];
+#pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) {
+      const unsigned bal = __ballot_sync(0xffffffffu, (sm >> l) & 1u);
+      excl[l] = run[l] + __popc(bal & lt);
+      run[l] += __popc(bal);
+    }
+    excl[kMaxLevels] = 0;
+    if (lam == 0) continue;
+#pragma unroll
+    for (int l = 0; l < kMaxLevels; ++l) {
+      const int started = (int)((sm >> l) & 1u);
+      if (started) {
+        const int b = s_base[l] + excl[l];
+        if (b < s_base[l + 1]) ws.lo_first[b] = make_int4(g, s_base[l + 1] + excl[l + 1], s_from, 0);
+        else record_error(sc, kStageLayout, 1);
+      }
+      if ((lm >> l) & 1u) {
+        const int b = s_base[l] + excl[l] + started - 1;
+        const int pre = s_from - lam + l - 1;
+        if (b >= s_base[l] && b < s_base[l + 1] && pre >= 0 && pre < M) ws.lo_last[b] = make_int2(g, pre);
+        else record_error(sc, kStageLayout, 1);
+      }
+    }
+  }
+}
+
+// The cells of one level (deepest first): mass and centre of mass from the
+// occupied leaf's particles in sorted order (octree_physics.cu:95-154) or
+// from the children's records in octant order (octree_physics.cu:156-245);
+// geometry from the key prefix (octree_geometry.cu:56-102); then the
+// traversal records at the preorder index (as layout_kernel writes them).
+template <int kRecords>
+__global__ void __launch_bounds__(kBlock) lo_level_kernel(Workspace ws, int level, double theta) {
+  __shared__ int s_lo, s_hi, s_end, s_g, s_m;
+  DevScalars *sc = ws.sc;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = 0, end = 0;
+    const int m = sc->n_nodes, g = sc->n_groups;
+    if (!sc->error && m > 0 && g > 0 && g <= ws.n) {
+      long long b = 0;
+      for (int l = 0; l < level; ++l) b += sc->level_count[l];
+      const long long h = b + sc->level_count[level];
+      const long long e = h + ((level + 1 < kMaxLevels) ? sc->level_count[level + 1] : 0);
+      if (e <= m) {
+        lo = (int)b;
+        hi = (int)h;
+        end = (int)e;
+      } else {
+        record_error(sc, kStageLayout, 1);
+      }
+    }
+    s_lo = lo;
+    s_hi = hi;
+    s_end = end;
+    s_g = g;
+    s_m = m;
+  }
+  __syncthreads();
+  const int lo = s_lo, hi = s_hi, end = s_end, G = s_g, M = s_m;
+  const int kb = ws.key_bits;
+  for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi; b += gridDim.x * blockDim.x) {
+    const int4 f = ws.lo_first[b];
+    const int2 q = ws.lo_last[b];
+    const int gf = f.x, c0 = f.y, skip = f.z, gl = q.x, pre = q.y;
+    const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
+    if (gf < 0 || gl < gf || gl >= G || pre < 0 || pre >= M || skip <= pre || skip > M || c0 < hi ||
+        c1 < c0 || c1 > end || c1 - c0 > 8) {
+      record_error(sc, kStageLayout, 1);
+      continue;
+    }
+    const bool leaf = c0 == c1;
+    const int pf = ws.gfirst[gf];
+    const int pe = ws.glast[gl] + 1;
+    if ((leaf && gf != gl) || pf < 0 || pe <= pf || pe > ws.n) {
+      record_error(sc, kStageTraversal, 2);
+      continue;
+    }
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    const int nk = c1 - c0;
+    // children in visit order: octant 7 -> 0, the children in descending key order
+    int *kids = ws.node_kids + (size_t)pre * 8;
+    if (leaf) {
+      for (int i = pf; i < pe; ++i) {
+        const double4 p = ws.pm4[i];
+        tm = __dadd_rn(tm, p.w);
+        wx = __fma_rn(p.w, p.x, wx);
+        wy = __fma_rn(p.w, p.y, wy);
+        wz = __fma_rn(p.w, p.z, wz);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (c0 + j < c1) {
+          const LevelNode ch = ws.lo_node[c0 + j];
+          const double cm = ch.a.w;
+          tm = __dadd_rn(tm, cm);
+          wx = __fma_rn(cm, ch.a.x, wx);
+          wy = __fma_rn(cm, ch.a.y, wy);
+          wz = __fma_rn(cm, ch.a.z, wz);
+          kids[nk - 1 - j] = ch.pre;
+        }
+      }
+    }
+    double comx = 0.0, comy = 0.0, comz = 0.0;
+    if (tm > 0.0) {
+      const double inv = __ddiv_rn(1.0, tm);
+      comx = __dmul_rn(wx, inv);
+      comy = __dmul_rn(wy, inv);
+      comz = __dmul_rn(wz, inv);
+    }
+    const double4 a = make_double4(comx, comy, comz, tm);
+    LevelNode rec;
+    rec.a = a;
+    rec.pre = pre;
+    rec.np = pe - pf;
+    rec.first = pf;
+    rec.leaf = leaf ? 1 : 0;
+    ws.lo_node[b] = rec;
+    // geometry
+    const unsigned long long key = ws.ukey[gf];
+    double cx = 0.0, cy = 0.0, cz = 0.0, h = 0.0;
+    if (level >= ws.sys_levels) {
+      const unsigned long long sys = key >> kSpatialBits;
+      if (sys >= (unsigned long long)ws.n_systems) {
+        record_error(sc, kStageGeometry, 2);
+        continue;
+      }
+      const double *box = ws.sys_box + 4 * (size_t)sys;
+      cx = box[0];
+      cy = box[1];
+      cz = box[2];
+      h = __dmul_rn(box[3], 0.5);
+      for (int d = ws.sys_levels + 1; d <= level; ++d) {
+        const int oct = (int)((key >> (kb - d * kDims)) & 7ull);
+        const double ch = __dmul_rn(h, 0.5);
+        cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
+        cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
+        cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
+        h = ch;
+      }
+      if (level == ws.sys_levels) ws.root_pre[sys] = pre;
+      if (!(h > 0.0)) record_error(sc, kStageTraversal, 8);
+    }
+    // traversal records
+    const double side = __dmul_rn(2.0, h);
+    const double ox = __dsub_rn(comx, cx), oy = __dsub_rn(comy, cy), oz = __dsub_rn(comz, cz);
+    const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
+    const double crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
+    const double c2 = __dmul_rn(crit, crit);
+    const double inner = __fma_rn(1.7320508075688774, h, __dsqrt_rn(o2));
+    const double cm = fmax(crit, inner) * (1.0 + 0x1p-40);
+    for (int j = nk; j < 8; ++j) kids[j] = -1;
+    if (kRecords & kRecordsFp64) {
+      ws.node_a[pre] = a;
+      ws.node_b[pre] = make_double4(cx, cy, cz, h);
+      ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), cm * cm);
+      ws.node_meta[pre] = make_int4(skip, leaf ? pf : -1, leaf ? pe - pf : 0, nk);
+    }
+    if (kRecords & kRecordsMixed) {
+      MixedNode mrec;
+      mrec.a = a;
+      mrec.cr2 = __double2float_ru(cm * cm * (1.0 + 0x1p-18));
+      mrec.first = leaf ? pf : -1;
+      mrec.count = leaf ? pe - pf : 0;
+      mrec.nchild = nk;
+      ws.node_m[pre] = mrec;
+    }
+  }
+}
+
+// Target-group starts on the level-order octree: group_mark_kernel's rule
+// with the children read as consecutive entries of the next level.
+__global__ void __launch_bounds__(kBlock) lo_group_mark_kernel(Workspace ws) {
+  __shared__ int s_base[kMaxLevels + 2];
+  __shared__ int s_m;
+  DevScalars *sc = ws.sc;
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int l = 0; l < kMaxLevels; ++l) {
+      s_base[l] = run;
+      run += sc->level_count[l];
+    }
+    s_base[kMaxLevels] = s_base[kMaxLevels + 1] = run;
+    s_m = (sc->error || sc->n_nodes != run) ? 0 : run;
+  }
+  __syncthreads();
+  const int M = s_m, gmax = ws.group_max, n = ws.n;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < M; b += gridDim.x * blockDim.x) {
+    int level = 0;
+    while (level + 1 < kMaxLevels && b >= s_base[level + 1]) ++level;
+    const LevelNode nd = ws.lo_node[b];
+    const int np = nd.np;
+    const bool virt = level < ws.sys_levels;  // children are other systems
+    const bool compact = !virt && (nd.leaf || np <= 1 || level - ws.sys_levels >= ws.group_depth);
+    if (!virt && np <= gmax && compact) {
+      // a whole system that is one group
+      if (level == ws.sys_levels && np > 0 && nd.first >= 0 && nd.first < n) ws.tflag[nd.first] = 1;
+      continue;
+    }
+    if (nd.leaf) {
+      // an occupied leaf with more than group_max coincident-key particles
+      for (int k = 0; k < np; k += gmax)
+        if (nd.first + k >= 0 && nd.first + k < n) ws.tflag[nd.first + k] = 1;
+      continue;
+    }
+    const int hi = s_base[level + 1], end = s_base[level + 2];
+    const int c0 = ws.lo_first[b].y;
+    const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
+    if (c0 < hi || c1 < c0 || c1 > end || c1 - c0 > 8) {
+      record_error(sc, kStageLayout, 1);
+      continue;
+    }
+    const bool merge = compact;  // split for its count only
+    int run = 0;
+    for (int c = c0; c < c1; ++c) {
+      const LevelNode ch = ws.lo_node[c];
+      const int cp = ch.np;
+      if (virt) run = 0;
+      const bool ccompact = ch.leaf || cp <= 1 || level + 1 - ws.sys_levels >= ws.group_depth;
+      if (cp > gmax || !ccompact) {
+        // the child splits itself
+        run = 0;
+        continue;
+      }
+      if (!merge || run == 0 || run + cp > gmax) {
+        if (ch.first >= 0 && ch.first < n) ws.tflag[ch.first] = 1;
+        run = 0;
+      }
+      run += cp;
+    }
+  }
+}
+
+// Reset of the counters the reference-numbered octree build uses, so that it
+// can run after a level-order build of the same step (tree export).
+__global__ void reference_octree_reset_kernel(DevScalars *sc) {
+  if (threadIdx.x == 0) {
+    sc->tile_counter[kTilePlan] = 0;
+    sc->tile_counter[kTileEnds] = 0;
+    for (int l = 0; l < kMaxLevels; ++l) sc->level_count[l] = 0;
+  }
+}
+
 // Reset the traversal counters and target-group scan state so the groups can
 // be rebuilt with another group size on an unchanged tree.
 __global__ void retarget_reset_kernel(DevScalars *sc) {
@@ -1538,7 +2007,8 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
+// Karras tree .. traversal layout in the reference's octree numbering.
+static cudaError_t launch_reference_body(Workspace &ws, double theta, cudaStream_t s) {
   const int grid = grid_for(ws, 8);
   karras_kernel<<<grid, kBlock, 0, s>>>(ws);
   plan_kernel<<<ws.scan_tiles_r, kScanThreads, 0, s>>>(ws);
@@ -1554,10 +2024,54 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
   ends_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   preorder_kernel<<<grid, kBlock, 0, s>>>(ws);
   layout_kernel<<<grid, kBlock, 0, s>>>(ws, theta);
+  count_launches(10 + (ws.max_level + 1));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
+  cudaError_t e = launch_reference_body(ws, theta, s);
+  if (e != cudaSuccess) return e;
+  const int grid = grid_for(ws, 8);
   group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(12 + (ws.max_level + 1));
+  count_launches(2);
   return cudaGetLastError();
+}
+
+cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s) {
+  if (!ws.lo_tiles) return cudaErrorInvalidValue;
+  const int grid = grid_for(ws, 8);
+  lo_span_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  lo_tile_scan_kernel<<<1, 32 * kLevelOrderChannels, 0, s>>>(ws);
+  lo_rank_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  for (int level = ws.max_level; level >= 0; --level) {
+    if (ws.records == kRecordsMixed)
+      lo_level_kernel<kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
+    else if (ws.records == kRecordsFp64)
+      lo_level_kernel<kRecordsFp64><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
+    else
+      lo_level_kernel<kRecordsFp64 | kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
+  }
+  lo_group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
+  count_launches(5 + (ws.max_level + 1));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_octree(Workspace &ws, double theta, cudaStream_t s) {
+  return ws.level_order ? launch_level_order_tree(ws, theta, s) : launch_tree(ws, theta, s);
+}
+
+cudaError_t launch_reference_octree(Workspace &ws, double theta, cudaStream_t s) {
+  reference_octree_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
+  count_launches(1);
+  cudaError_t e = cudaMemsetAsync(ws.scan_status + ws.scan_tiles_n, 0,
+                                  sizeof(unsigned long long) * (size_t)ws.scan_tiles_r, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(ws.scan_status + 2 * ws.scan_tiles_n + ws.scan_tiles_r, 0,
+                      sizeof(unsigned long long) * (size_t)ws.scan_tiles_n, s);
+  if (e != cudaSuccess) return e;
+  return launch_reference_body(ws, theta, s);
 }
 
 cudaError_t launch_morton_sort_only(Workspace &ws, uint32_t *keys, uint32_t *idx, cudaStream_t s) {
@@ -1601,7 +2115,10 @@ cudaError_t launch_retarget(Workspace &ws, cudaStream_t s) {
                       sizeof(unsigned long long) * (size_t)ws.scan_tiles_n, s);
   if (e != cudaSuccess) return e;
   const int grid = grid_for(ws, 8);
-  group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  if (ws.level_order)
+    lo_group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  else
+    group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   count_launches(3);
   return cudaGetLastError();

@@ -168,7 +168,8 @@ struct Allocation {
 
 // Allocate every buffer of a workspace for n particles (state included when
 // with_state).  All device memory is taken here; nothing is allocated later.
-cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_state, int n_systems = 1) {
+cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_state, int n_systems = 1,
+                            bool level_order = false) {
   ws = Workspace{};
   ws.n = n;
   ws.n_systems = n_systems;
@@ -221,6 +222,12 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   GET(ws.node_a, C); GET(ws.node_b, C); GET(ws.node_c, C); GET(ws.node_meta, C);
   GET(ws.node_kids, 8 * C);
   GET(ws.node_m, C);
+  if (level_order) {
+    ws.level_order = 1;
+    GET(ws.gspan, N);
+    GET(ws.lo_first, C); GET(ws.lo_last, C); GET(ws.lo_node, C);
+    GET(ws.lo_tiles, (size_t)ws.scan_tiles_n * kLevelOrderChannels);
+  }
 #undef GET
   e = cudaMemset(ws.sc, 0, sizeof(DevScalars));
   if (e != cudaSuccess) return e;
@@ -320,6 +327,8 @@ int check_device(const Workspace &ws, cudaStream_t s) {
 cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, double dt, int kd,
                                   cudaStream_t s, int part = 0) {
   ws.group_max = (tp.group_mode && tp.group_size > 32) ? (tp.group_size > 64 ? 128 : 64) : 32;
+  // the level-order build writes only the records of this walk
+  ws.records = tp.precision == NBB_PRECISION_MIXED ? kRecordsMixed : kRecordsFp64;
   cudaError_t e = cudaSuccess;
   if (part == 0 || part == 1) {
     e = launch_step_reset(ws, s);
@@ -327,7 +336,7 @@ cudaError_t enqueue_rebuild_force(Workspace &ws, const TraversalParams &tp, doub
   }
   if (e == cudaSuccess && part != 1) e = launch_morton_sort_groups(ws, s, part == 0 ? 0 : part - 1);
   if (part == 1 || part == 2) return e;
-  if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
+  if (e == cudaSuccess) e = launch_octree(ws, tp.theta, s);
   if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
   return e;
 }
@@ -532,7 +541,7 @@ static int create_sim(const nbb_config *cfg, size_t n, int n_systems, const int6
   sim->cfg = *cfg;
   sim->min_softening = min_eps;
   cudaError_t e = cudaStreamCreateWithFlags(&sim->own_stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = alloc_workspace(sim->ws, sim->alloc, (int)n, true, n_systems > 1 ? n_systems : 1);
+  if (e == cudaSuccess) e = alloc_workspace(sim->ws, sim->alloc, (int)n, true, n_systems > 1 ? n_systems : 1, true);
   if (e != cudaSuccess) {
     if (sim->own_stream) cudaStreamDestroy(sim->own_stream);
     delete sim;
@@ -1026,7 +1035,7 @@ int nbb_sim_profile(nbb_sim *sim, float *stage_ms, nbb_stats *stats) {
   if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
   if (e == cudaSuccess) e = launch_morton_sort_groups(ws, s);
   if (e == cudaSuccess) e = cudaEventRecord(ev[3], s);
-  if (e == cudaSuccess) e = launch_tree(ws, tp.theta, s);
+  if (e == cudaSuccess) e = launch_octree(ws, tp.theta, s);
   if (e == cudaSuccess) e = cudaEventRecord(ev[4], s);
   if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
   if (e == cudaSuccess) e = cudaEventRecord(ev[5], s);
@@ -1050,6 +1059,13 @@ int nbb_sim_export(nbb_sim *sim, nbb_tree_export *out) {
   if (!sim || !out) return fail(NBB_ERR_INVALID_ARGUMENT, "null argument");
   if (sim->state == nbb_sim::State::created)
     return fail(NBB_ERR_LOGIC, "Simulation spatial/device state is not available");
+  if (sim->ws.level_order && sim->state == nbb_sim::State::ready) {
+    // the steps build the level-order octree: the reference-numbered arrays
+    // of the exported tree are rebuilt from the last build's leaf groups
+    NBB_CUDA(launch_reference_octree(sim->ws, traversal_params(sim, 0).theta, sim->stream), "tree export");
+    const int st = check_device(sim->ws, sim->stream);
+    if (st) return st;
+  }
   return export_workspace(sim->ws, out, sim->stream, true);
 }
 
@@ -1826,6 +1842,8 @@ int nbb_frozen_rollout(const nbb_config *cfg, size_t n, const double *mass, cons
   int st = create_sim(&c2, n, 1, nullptr, nullptr, mass, x, y, z, vx, vy, vz, nullptr, on_device, &sim);
   if (st) return st;
   std::unique_ptr<nbb_sim, int (*)(nbb_sim *)> guard(sim, nbb_sim_destroy);
+  // the frozen walk reads the octree in the reference numbering
+  sim->ws.level_order = 0;
   st = nbb_sim_initialize(sim);
   if (st) return st;
   Workspace &ws = sim->ws;

@@ -97,6 +97,28 @@ struct __align__(16) MixedNode {
 };
 static_assert(sizeof(MixedNode) == 48, "two 32-byte sectors per node");
 
+// A node of the level-order octree (the step's build): the same octree as
+// the reference's, numbered level by level with each level in ascending key
+// order, so that a node's children are consecutive entries of the next level.
+struct __align__(16) LevelNode {
+  double4 a;  // com x, y, z, mass
+  int pre;    // depth-first preorder index (children visited octant 7 -> 0)
+  int np;     // particles in the subtree
+  int first;  // first particle of the subtree (sorted order)
+  int leaf;   // 1 for an occupied leaf
+};
+static_assert(sizeof(LevelNode) == 48, "two 32-byte sectors per node");
+
+// Per-tile counts of the level-order build (tiles of kScanTile groups): the
+// cells started per octree level, then the cells ended (kMaxLevels); the
+// rest pad a warp.
+constexpr int kLevelOrderChannels = 32;
+
+// Traversal records a build writes: the plain FP64 walk's (node_a, node_b,
+// node_c, node_meta) and the mixed walk's (node_m); child lists always.
+constexpr int kRecordsFp64 = 1;
+constexpr int kRecordsMixed = 2;
+
 // Everything a spatial rebuild and a traversal touch, sized for capacity n.
 struct Workspace {
   int n = 0;            // particle count
@@ -182,6 +204,15 @@ struct Workspace {
   int4 *node_meta = nullptr;  // skip, first particle, particle count, nchild
   int *node_kids = nullptr;   // 8 per node, preorder ids in visit order
   MixedNode *node_m = nullptr;  // the mixed walk's records, preorder
+
+  // level-order build (simulation steps): the octree numbered level by level
+  int level_order = 0;          // host: 1 when steps build the level-order octree
+  int *gspan = nullptr;         // n: per group (delta + 1) | lambda << 8 | (delta_next + 1) << 16
+  int4 *lo_first = nullptr;     // cap: first group, first child, subtree end (preorder)
+  int2 *lo_last = nullptr;      // cap: last group, preorder index
+  LevelNode *lo_node = nullptr;  // cap: mass, centre of mass, preorder index, particles
+  int *lo_tiles = nullptr;      // scan_tiles_n * kLevelOrderChannels: per-tile counts, then their prefixes
+  int records = kRecordsFp64 | kRecordsMixed;  // host: the records the level-order build writes
   int *walk_ext = nullptr;    // walk_warps x walk_ext_cap: the mixed walk's stack below shared memory
 };
 
@@ -273,6 +304,15 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part = 
 // Karras tree, plan + scan, octree materialisation, geometry, physics,
 // preorder layout.
 cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s);
+// The same octree built level by level from the sorted unique keys (no radix
+// tree), with the same traversal records and target groups; needs the
+// level-order arrays of the workspace.
+cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s);
+// launch_level_order_tree when ws.level_order, else launch_tree.
+cudaError_t launch_octree(Workspace &ws, double theta, cudaStream_t s);
+// The reference-numbered octree (Karras .. layout, no target groups) over the
+// current leaf groups, after a level-order build of the same step (export).
+cudaError_t launch_reference_octree(Workspace &ws, double theta, cudaStream_t s);
 // Rebuild the octree target groups for ws.group_max on the current tree and
 // reset the traversal counters (used by the group-size autotuner).
 cudaError_t launch_retarget(Workspace &ws, cudaStream_t s);

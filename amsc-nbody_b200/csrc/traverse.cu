@@ -227,7 +227,7 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
 
 // Evaluate `count` list entries (rounded up to a whole pair; an odd count
 // has a zero-mass pad after it) for this lane's kTPL targets: FP32 offsets,
-// approximate rsqrt plus one Newton step, two-wide FP32 partial sums over
+// approximate rsqrt (no refinement), two-wide FP32 partial sums over
 // the batch, then one Kahan-compensated addition of each batch partial into
 // its running sum.
 //
@@ -257,7 +257,6 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
   float2 px[kTPL], py[kTPL], pz[kTPL];
 #pragma unroll
   for (int q = 0; q < kTPL; ++q) px[q] = py[q] = pz[q] = make_float2(0.f, 0.f);
-  const float2 minus_three_halves = make_float2(-1.5f, -1.5f), five_halves = make_float2(2.5f, 2.5f);
   bool singular = false;
   const int pairs = (count + 1) >> 1;
 #pragma unroll kUnroll
@@ -270,11 +269,12 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
       const float2 dx = __fadd2_rn(ex, ntx[q]), dy = __fadd2_rn(ey, nty[q]), dz = __fadd2_rn(ez, ntz[q]);
       const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
       const float2 r = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-      // one Newton step for z = r2^(-3/2) from z0 = r^3 (Newton's method on
-      // z^(-2/3) - r2 = 0): z = z0 (5/2 - 3/2 r2 r^2)
+      // m r^-3 straight from the hardware estimate: its relative error (a few
+      // 1e-7 on r^-3) sits far below the Barnes-Hut truncation error this
+      // form is held to, and a Newton step would add 3 packed FP32 operations
+      // to the 12 of a pair of entries
       const float2 rr = __fmul2_rn(r, r);
-      const float2 c = __ffma2_rn(__fmul2_rn(r2, rr), minus_three_halves, five_halves);
-      float2 f = __fmul2_rn(__fmul2_rn(em, c), __fmul2_rn(rr, r));
+      float2 f = __fmul2_rn(__fmul2_rn(em, r), rr);
       if (kTrackSource) {
         const bool o0 = src[2 * pr] != self[q], o1 = src[2 * pr + 1] != self[q];
         singular |= (o0 && !(r2.x > 0.f) && em.x != 0.f) || (o1 && !(r2.y > 0.f) && em.y != 0.f);
