@@ -335,11 +335,13 @@ constexpr uint32_t kDigitFlagP = 2u << 30;  // inclusive prefix published
 constexpr uint32_t kDigitMask = (1u << 30) - 1u;
 
 // One stable LSD pass over 8 key bits.  A tile's items are ranked warp by
-// warp and round by round in input order (match_any groups equal digits in a
-// round), so equal digits keep their input order: the result is the stable
-// order of thrust::stable_sort_by_key.  Tile prefixes per digit come from a
-// decoupled look-back over the tiles launched before it (tile ids are taken
-// from an atomic counter, so every predecessor is already running).  The
+// warp and round by round in input order (the lanes holding the same digit in
+// a round are found with one ballot per digit bit, a cost that does not grow
+// with the number of distinct digits), so equal digits keep their input
+// order: the result is the stable order of thrust::stable_sort_by_key.  Tile
+// prefixes per digit come from a decoupled look-back over the tiles launched
+// before it (tile ids are taken from an atomic counter, so every predecessor
+// is already running), reading 16 predecessors' status words at once.  The
 // ranked tile is first placed in shared memory in digit order, then written
 // out by consecutive threads: a digit's items of one tile land at consecutive
 // addresses, so the stores go out as runs instead of one scattered 8-byte
@@ -376,7 +378,15 @@ __global__ void __launch_bounds__(kSortThreads)
     const int i = start + it * 32 + lane;
     const bool valid = i < n;
     const uint32_t dig = (uint32_t)(key[it] >> shift) & 255u;
-    const unsigned peers = __match_any_sync(0xffffffffu, valid ? dig : 0xFFFFFFFFu);
+    // lanes with the same digit (bit 8 marks the items past the end)
+    const uint32_t code = valid ? dig : 256u;
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) {
+      const bool bit = (code >> b) & 1u;
+      const unsigned on = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? on : ~on;
+    }
     uint32_t base = 0;
     if (valid) base = whist[warp][dig];
     __syncwarp();
@@ -387,53 +397,31 @@ __global__ void __launch_bounds__(kSortThreads)
     __syncwarp();
   }
   __syncthreads();
-  {
-    // digit tid: offsets of the warps' runs, the tile's count, its place in
-    // the staged tile (exclusive scan over digits) and its output base
-    uint32_t run = 0;
+  // digit tid: offsets of the warps' runs, the tile's count (published at
+  // once), its place in the staged tile (exclusive scan over digits)
+  uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const uint32_t c = whist[w][tid];
-      whist[w][tid] = run;
-      run += c;
-    }
+  for (int w = 0; w < kWarps; ++w) {
+    const uint32_t c = whist[w][tid];
+    whist[w][tid] = run;
+    run += c;
+  }
+  uint32_t *my = status + (size_t)tile * 256 + tid;
+  st_release_u32(my, (tile == 0 ? kDigitFlagP : kDigitFlagA) | run);
+  {
     uint32_t inc = run;
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += v;
     }
     if (lane == 31) warp_tot[warp] = inc;
-    uint32_t *my = status + (size_t)tile * 256 + tid;
-    uint32_t prefix = 0;
-    if (tile == 0) {
-      st_release_u32(my, kDigitFlagP | run);
-    } else {
-      st_release_u32(my, kDigitFlagA | run);
-      int j = tile - 1;
-      int spins = 0;
-      while (j >= 0) {
-        const uint32_t st = ld_acquire_u32(status + (size_t)j * 256 + tid);
-        const uint32_t flag = st & ~kDigitMask;
-        if (flag == 0u) {
-          if (++spins > kSpinLimit) {
-            record_error(sc, kStageSort, kCodeTimeout);
-            break;
-          }
-          continue;
-        }
-        prefix += st & kDigitMask;
-        if (flag == kDigitFlagP) break;
-        --j;
-      }
-      st_release_u32(my, kDigitFlagP | (prefix + run));
-    }
     __syncthreads();
     uint32_t wbase = 0;
     for (int w = 0; w < warp; ++w) wbase += warp_tot[w];
     tile_excl[tid] = wbase + inc - run;
-    digit_base[tid] = digit_offsets[pass * 256 + tid] + prefix;
   }
   __syncthreads();
+  // the tile in digit order in shared memory, while the predecessors publish
 #pragma unroll
   for (int it = 0; it < kSortItems; ++it) {
     const int i = start + it * 32 + lane;
@@ -442,6 +430,46 @@ __global__ void __launch_bounds__(kSortThreads)
       const uint32_t local = tile_excl[dig] + whist[warp][dig] + rank[it];
       if (local < (uint32_t)kSortTile) stage[local] = key[it];
     }
+  }
+  {
+    // digit tid: the tile's output base from the look-back
+    uint32_t prefix = 0;
+    if (tile > 0) {
+      // predecessors j, j-1, ..., read kLookWindow at a time: aggregates are
+      // added until an inclusive prefix (added too); an unpublished word
+      // ends the window and is read again
+      constexpr int kLookWindow = 32;
+      int j = tile - 1;
+      int spins = 0;
+      bool done = false;
+      while (!done) {
+        uint32_t st[kLookWindow];
+#pragma unroll
+        for (int w = 0; w < kLookWindow; ++w)
+          st[w] = (j - w >= 0) ? ld_relaxed_u32(status + (size_t)(j - w) * 256 + tid) : kDigitFlagP;
+        int used = 0;
+        bool stop = false;
+#pragma unroll
+        for (int w = 0; w < kLookWindow; ++w) {
+          if (stop) continue;
+          const uint32_t flag = st[w] & ~kDigitMask;
+          if (flag == 0u) {
+            stop = true;
+          } else {
+            prefix += st[w] & kDigitMask;
+            ++used;
+            if (flag == kDigitFlagP) stop = done = true;
+          }
+        }
+        j -= used;
+        if (!done && used == 0 && ++spins > kSpinLimit) {
+          record_error(sc, kStageSort, kCodeTimeout);
+          break;
+        }
+      }
+      st_release_u32(my, kDigitFlagP | (prefix + run));
+    }
+    digit_base[tid] = digit_offsets[pass * 256 + tid] + prefix;
   }
   __syncthreads();
   const int count = min(kSortTile, n - tile * kSortTile);
@@ -1487,31 +1515,57 @@ __global__ void __launch_bounds__(kScanThreads) lo_span_kernel(Workspace ws) {
     ws.lo_tiles[(size_t)blockIdx.x * kLevelOrderChannels + threadIdx.x] = s_cnt[threadIdx.x];
 }
 
-// Exclusive prefixes of the per-tile counts, one warp per channel, in place;
-// the totals give the cells per level and M (the node count).
+// Exclusive prefixes of the per-tile counts, in place, through shared memory:
+// chunks of tiles are loaded with coalesced reads, each warp scans one
+// channel of the chunk (a lane holds 8 consecutive tiles), and the chunk is
+// written back coalesced.  The totals give the cells per level and M (the
+// node count).
 __global__ void __launch_bounds__(32 * kLevelOrderChannels) lo_tile_scan_kernel(Workspace ws) {
   constexpr int kEnded = kMaxLevels;
+  constexpr int kPerLane = 8;
+  constexpr int kChunk = 32 * kPerLane;  // tiles per chunk
+  __shared__ int s_cnt[kChunk][kLevelOrderChannels + 1];
   __shared__ long long s_total[kLevelOrderChannels];
   DevScalars *sc = ws.sc;
   const int g = sc->n_groups;
   const int G = (g > 0 && g <= ws.n) ? g : 0;
   const int tiles = (G + kScanTile - 1) / kScanTile;
   const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  long long carry = 0;
-  for (int t0 = 0; t0 < tiles; t0 += 32) {
-    const int t = t0 + lane;
-    int *p = ws.lo_tiles + (size_t)t * kLevelOrderChannels + c;
-    const int v = (t < tiles) ? *p : 0;
-    int inc = v;
+  int inc = 0;  // running total of channel c
+  for (int t0 = 0; t0 < tiles; t0 += kChunk) {
+    const int nt = min(kChunk, tiles - t0);
+    const int *src = ws.lo_tiles + (size_t)t0 * kLevelOrderChannels;
+    for (int i = threadIdx.x; i < nt * kLevelOrderChannels; i += blockDim.x)
+      s_cnt[i / kLevelOrderChannels][i % kLevelOrderChannels] = src[i];
+    __syncthreads();
+    int v[kPerLane], sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPerLane; ++j) {
+      const int t = lane * kPerLane + j;
+      v[j] = (t < nt) ? s_cnt[t][c] : 0;
+      sum += v[j];
+    }
+    int x = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int u = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += u;
+      const int u = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += u;
     }
-    if (t < tiles) *p = (int)(carry + inc - v);
-    carry += __shfl_sync(0xffffffffu, inc, 31);
+    int acc = inc + x - sum;
+#pragma unroll
+    for (int j = 0; j < kPerLane; ++j) {
+      const int t = lane * kPerLane + j;
+      if (t < nt) s_cnt[t][c] = acc;
+      acc += v[j];
+    }
+    inc += __shfl_sync(0xffffffffu, x, 31);
+    __syncthreads();
+    int *dst = ws.lo_tiles + (size_t)t0 * kLevelOrderChannels;
+    for (int i = threadIdx.x; i < nt * kLevelOrderChannels; i += blockDim.x)
+      dst[i] = s_cnt[i / kLevelOrderChannels][i % kLevelOrderChannels];
+    __syncthreads();
   }
-  if (lane == 0) s_total[c] = carry;
+  if (lane == 0) s_total[c] = inc;
   __syncthreads();
   if (threadIdx.x == 0) {
     long long m = 0;
@@ -1528,17 +1582,101 @@ __global__ void __launch_bounds__(32 * kLevelOrderChannels) lo_tile_scan_kernel(
   }
 }
 
+// One cell's records from its mass sums: the LevelNode its parent reads, the
+// geometry from the key prefix (octree_geometry.cu:56-102) and the traversal
+// records at the preorder index (as layout_kernel writes them).  The child
+// list is the caller's.  Neither walk applies the acceptance test to an
+// occupied leaf (its particles are summed), so a leaf gets no geometry and no
+// acceptance radius.  Returns false on an invalid system id.
+template <int kRecords>
+__device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double theta, int b, int pre, int skip,
+                                        int pf, int pe, bool leaf, int nk, double tm, double wx, double wy,
+                                        double wz, unsigned long long key) {
+  double comx = 0.0, comy = 0.0, comz = 0.0;
+  if (tm > 0.0) {
+    const double inv = __ddiv_rn(1.0, tm);
+    comx = __dmul_rn(wx, inv);
+    comy = __dmul_rn(wy, inv);
+    comz = __dmul_rn(wz, inv);
+  }
+  const double4 a = make_double4(comx, comy, comz, tm);
+  LevelNode rec;
+  rec.a = a;
+  rec.pre = pre;
+  rec.np = pe - pf;
+  rec.first = pf;
+  rec.leaf = leaf ? 1 : 0;
+  ws.lo_node[b] = rec;
+  double cx = 0.0, cy = 0.0, cz = 0.0, h = 0.0;
+  if (level >= ws.sys_levels) {
+    const unsigned long long sys = key >> kSpatialBits;
+    if (sys >= (unsigned long long)ws.n_systems) return false;
+    if (level == ws.sys_levels) ws.root_pre[sys] = pre;
+  }
+  if (level >= ws.sys_levels && !leaf) {
+    const unsigned long long sys = key >> kSpatialBits;
+    const double *box = ws.sys_box + 4 * (size_t)sys;
+    cx = box[0];
+    cy = box[1];
+    cz = box[2];
+    h = __dmul_rn(box[3], 0.5);
+    const int kb = ws.key_bits;
+    for (int d = ws.sys_levels + 1; d <= level; ++d) {
+      const int oct = (int)((key >> (kb - d * kDims)) & 7ull);
+      const double ch = __dmul_rn(h, 0.5);
+      cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
+      cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
+      cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
+      h = ch;
+    }
+    if (!(h > 0.0)) record_error(ws.sc, kStageTraversal, 8);
+  }
+  double crit = 0.0, c2 = 0.0, cm = 0.0;
+  if (!leaf) {
+    const double side = __dmul_rn(2.0, h);
+    const double ox = __dsub_rn(comx, cx), oy = __dsub_rn(comy, cy), oz = __dsub_rn(comz, cz);
+    const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
+    crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
+    c2 = __dmul_rn(crit, crit);
+    const double inner = __fma_rn(1.7320508075688774, h, __dsqrt_rn(o2));
+    cm = fmax(crit, inner) * (1.0 + 0x1p-40);
+  }
+  if (kRecords & kRecordsFp64) {
+    ws.node_a[pre] = a;
+    if (!leaf) {
+      ws.node_b[pre] = make_double4(cx, cy, cz, h);
+      ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), cm * cm);
+    }
+    ws.node_meta[pre] = make_int4(skip, leaf ? pf : -1, leaf ? pe - pf : 0, nk);
+  }
+  if (kRecords & kRecordsMixed) {
+    MixedNode mrec;
+    mrec.a = a;
+    mrec.cr2 = leaf ? 0.f : __double2float_ru(cm * cm * (1.0 + 0x1p-18));
+    mrec.first = leaf ? pf : -1;
+    mrec.count = leaf ? pe - pf : 0;
+    mrec.nchild = nk;
+    ws.node_m[pre] = mrec;
+  }
+  return true;
+}
+
 // Cell numbers: per tile, the cells started by the groups before it (the
 // tile prefixes) plus the ranks inside the tile.  Writes each cell's first
-// group, first child and subtree end (by its first group) and its last group
-// and preorder index (by its last group).
-__global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
+// particle, first child, subtree end and first group (by its first group) and
+// its particle end, preorder index and key (by its last group; every group of
+// a cell carries the cell's prefix).  A group's leaf (level lambda, preorder
+// index S(g) - 1) is finished here: mass and centre of mass of its particles
+// in sorted order (octree_physics.cu:95-154) and its records.
+template <int kRecords>
+__global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, double theta) {
   constexpr int kWarps = kScanThreads / 32;
   constexpr int kNodes = kMaxLevels;  // channel of the ended cells (the node count S)
   static_assert(kNodes < kLevelOrderChannels, "one warp holds every channel");
   __shared__ int s_warp[kWarps][kLevelOrderChannels];
   __shared__ int s_prefix[kLevelOrderChannels];
   __shared__ int s_base[kMaxLevels + 2];
+  __shared__ int s_span[kScanItems][kScanThreads];
   __shared__ int s_g, s_m;
   DevScalars *sc = ws.sc;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1563,11 +1701,10 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
   // each warp owns 32 * kScanItems consecutive groups, item k at g0 + 32 k;
   // a group's cells: started at levels (delta, lambda], ended at (delta_next, lambda]
   const int g0 = base + warp * (32 * kScanItems) + lane;
-  auto masks = [&](int g, unsigned &smask, unsigned &lmask, int &lam) {
+  auto masks = [&](int sp, unsigned &smask, unsigned &lmask, int &lam) {
     smask = lmask = 0u;
     lam = 0;
-    if (g >= G) return;
-    const int sp = ws.gspan[g];
+    if (sp < 0) return;
     const int d = (sp & 255) - 1, l = (sp >> 8) & 255, dn = ((sp >> 16) & 255) - 1;
     if (l < 1 || l > max_level || d >= l || dn >= l) {
       record_error(sc, kStagePlan, 3);
@@ -1578,20 +1715,40 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
     lmask = upto & ~((1u << (dn + 1)) - 1u);
     lam = l;
   };
+  // the spans, all loads in flight at once; kept in shared memory for the
+  // second pass
+  int span[kScanItems];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int g = g0 + 32 * k;
+    span[k] = (g < G) ? ws.gspan[g] : -1;
+  }
   // this warp's cells per level (lane l) and node count (lane kNodes)
   int cnt[kMaxLevels];
 #pragma unroll
   for (int l = 0; l < kMaxLevels; ++l) cnt[l] = 0;
   int e = 0;
-#pragma unroll 1
+#pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
+    s_span[k][tid] = span[k];
     unsigned sm, lm;
     int lam;
-    masks(g0 + 32 * k, sm, lm, lam);
+    masks(span[k], sm, lm, lam);
 #pragma unroll
     for (int l = 0; l < kMaxLevels; ++l) cnt[l] += (int)((sm >> l) & 1u);
     e += __popc(lm);
   }
+  // the warp's level range: ranks are formed only where its groups have cells
+  int wlo = kMaxLevels, whi = -1;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (span[k] < 0) continue;
+    const int d = (span[k] & 255) - 1, l = (span[k] >> 8) & 255, dn = ((span[k] >> 16) & 255) - 1;
+    wlo = min(wlo, min(d, dn) + 1);
+    whi = max(whi, l + 1);
+  }
+  wlo = __reduce_min_sync(0xffffffffu, wlo);
+  whi = min(__reduce_max_sync(0xffffffffu, whi), kMaxLevels);
   int mine = __reduce_add_sync(0xffffffffu, e);
   mine = (lane == kNodes) ? mine : 0;
 #pragma unroll
@@ -1619,9 +1776,18 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
 #pragma unroll 1
   for (int k = 0; k < kScanItems; ++k) {
     const int g = g0 + 32 * k;
+    const int sp = s_span[k][tid];
+    // the cell payloads (read before the ranks are formed)
+    int pf = 0, pe = 0;
+    unsigned long long key = 0ull;
+    if (sp >= 0) {
+      pf = ws.gfirst[g];
+      pe = ws.glast[g] + 1;
+      key = ws.ukey[g];
+    }
     unsigned sm, lm;
     int lam;
-    masks(g, sm, lm, lam);
+    masks(sp, sm, lm, lam);
     const int ek = __popc(lm);
     int inc = ek;
 #pragma unroll
@@ -1634,43 +1800,67 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws) {
     int excl[kMaxLevels + 1];
 #pragma unroll
     for (int l = 0; l < kMaxLevels; ++l) {
+      excl[l] = 0;
+      if (l < wlo || l > whi) continue;  // warp-uniform
       const unsigned bal = __ballot_sync(0xffffffffu, (sm >> l) & 1u);
       excl[l] = run[l] + __popc(bal & lt);
       run[l] += __popc(bal);
     }
     excl[kMaxLevels] = 0;
     if (lam == 0) continue;
+    int bleaf = -1;
 #pragma unroll
     for (int l = 0; l < kMaxLevels; ++l) {
+      if (l < wlo || l > whi) continue;
       const int started = (int)((sm >> l) & 1u);
       if (started) {
         const int b = s_base[l] + excl[l];
-        if (b < s_base[l + 1]) ws.lo_first[b] = make_int4(g, s_base[l + 1] + excl[l + 1], s_from, 0);
+        if (b < s_base[l + 1]) ws.lo_first[b] = make_int4(pf, s_base[l + 1] + excl[l + 1], s_from, g);
         else record_error(sc, kStageLayout, 1);
+        if (l == lam) bleaf = b;
       }
-      if ((lm >> l) & 1u) {
+      if (((lm >> l) & 1u) && l < lam) {
         const int b = s_base[l] + excl[l] + started - 1;
         const int pre = s_from - lam + l - 1;
-        if (b >= s_base[l] && b < s_base[l + 1] && pre >= 0 && pre < M) ws.lo_last[b] = make_int2(g, pre);
-        else record_error(sc, kStageLayout, 1);
+        if (b >= s_base[l] && b < s_base[l + 1] && pre >= 0 && pre < M)
+          ws.lo_last[b] = make_int4(pe, pre, (int)(unsigned)key, (int)(unsigned)(key >> 32));
+        else
+          record_error(sc, kStageLayout, 1);
       }
     }
+    // the leaf: its particles in sorted order, its records at S(g) - 1
+    const int pre = s_from - 1;
+    if (bleaf < 0 || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n) {
+      record_error(sc, kStageLayout, 1);
+      continue;
+    }
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    for (int i = pf; i < pe; ++i) {
+      const double4 q = ws.pm4[i];
+      tm = __dadd_rn(tm, q.w);
+      wx = __fma_rn(q.w, q.x, wx);
+      wy = __fma_rn(q.w, q.y, wy);
+      wz = __fma_rn(q.w, q.z, wz);
+    }
+    int4 *kids = reinterpret_cast<int4 *>(ws.node_kids + (size_t)pre * 8);
+    kids[0] = make_int4(-1, -1, -1, -1);
+    kids[1] = make_int4(-1, -1, -1, -1);
+    if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, s_from, pf, pe, true, 0, tm, wx, wy, wz, key))
+      record_error(sc, kStageGeometry, 2);
   }
 }
 
-// The cells of one level (deepest first): mass and centre of mass from the
-// occupied leaf's particles in sorted order (octree_physics.cu:95-154) or
-// from the children's records in octant order (octree_physics.cu:156-245);
-// geometry from the key prefix (octree_geometry.cu:56-102); then the
-// traversal records at the preorder index (as layout_kernel writes them).
+// The internal cells of one level (deepest first; the leaves were finished
+// by lo_rank_kernel): mass and centre of mass from the children's records in
+// octant order (octree_physics.cu:156-245), then the cell's records.
 template <int kRecords>
-__global__ void __launch_bounds__(kBlock) lo_level_kernel(Workspace ws, int level, double theta) {
-  __shared__ int s_lo, s_hi, s_end, s_g, s_m;
+__global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int level, double theta) {
+  __shared__ int s_lo, s_hi, s_end, s_m;
   DevScalars *sc = ws.sc;
   if (threadIdx.x == 0) {
     int lo = 0, hi = 0, end = 0;
-    const int m = sc->n_nodes, g = sc->n_groups;
-    if (!sc->error && m > 0 && g > 0 && g <= ws.n) {
+    const int m = sc->n_nodes;
+    if (!sc->error && m > 0) {
       long long b = 0;
       for (int l = 0; l < level; ++l) b += sc->level_count[l];
       const long long h = b + sc->level_count[level];
@@ -1686,119 +1876,42 @@ __global__ void __launch_bounds__(kBlock) lo_level_kernel(Workspace ws, int leve
     s_lo = lo;
     s_hi = hi;
     s_end = end;
-    s_g = g;
     s_m = m;
   }
   __syncthreads();
-  const int lo = s_lo, hi = s_hi, end = s_end, G = s_g, M = s_m;
-  const int kb = ws.key_bits;
+  const int lo = s_lo, hi = s_hi, end = s_end, M = s_m;
   for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi; b += gridDim.x * blockDim.x) {
     const int4 f = ws.lo_first[b];
-    const int2 q = ws.lo_last[b];
-    const int gf = f.x, c0 = f.y, skip = f.z, gl = q.x, pre = q.y;
+    const int c0 = f.y;
     const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
-    if (gf < 0 || gl < gf || gl >= G || pre < 0 || pre >= M || skip <= pre || skip > M || c0 < hi ||
-        c1 < c0 || c1 > end || c1 - c0 > 8) {
+    if (c0 == c1) continue;  // a leaf
+    const int4 q = ws.lo_last[b];
+    const int pf = f.x, skip = f.z, pe = q.x, pre = q.y;
+    if (pre < 0 || pre >= M || skip <= pre + 1 || skip > M || c0 < hi || c1 < c0 || c1 > end || c1 - c0 > 8 ||
+        pf < 0 || pe <= pf || pe > ws.n) {
       record_error(sc, kStageLayout, 1);
       continue;
     }
-    const bool leaf = c0 == c1;
-    const int pf = ws.gfirst[gf];
-    const int pe = ws.glast[gl] + 1;
-    if ((leaf && gf != gl) || pf < 0 || pe <= pf || pe > ws.n) {
-      record_error(sc, kStageTraversal, 2);
-      continue;
-    }
-    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
     const int nk = c1 - c0;
     // children in visit order: octant 7 -> 0, the children in descending key order
     int *kids = ws.node_kids + (size_t)pre * 8;
-    if (leaf) {
-      for (int i = pf; i < pe; ++i) {
-        const double4 p = ws.pm4[i];
-        tm = __dadd_rn(tm, p.w);
-        wx = __fma_rn(p.w, p.x, wx);
-        wy = __fma_rn(p.w, p.y, wy);
-        wz = __fma_rn(p.w, p.z, wz);
-      }
-    } else {
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (c0 + j < c1) {
-          const LevelNode ch = ws.lo_node[c0 + j];
-          const double cm = ch.a.w;
-          tm = __dadd_rn(tm, cm);
-          wx = __fma_rn(cm, ch.a.x, wx);
-          wy = __fma_rn(cm, ch.a.y, wy);
-          wz = __fma_rn(cm, ch.a.z, wz);
-          kids[nk - 1 - j] = ch.pre;
-        }
+    for (int j = 0; j < 8; ++j) {
+      if (c0 + j < c1) {
+        const LevelNode ch = ws.lo_node[c0 + j];
+        const double cm = ch.a.w;
+        tm = __dadd_rn(tm, cm);
+        wx = __fma_rn(cm, ch.a.x, wx);
+        wy = __fma_rn(cm, ch.a.y, wy);
+        wz = __fma_rn(cm, ch.a.z, wz);
+        kids[nk - 1 - j] = ch.pre;
       }
     }
-    double comx = 0.0, comy = 0.0, comz = 0.0;
-    if (tm > 0.0) {
-      const double inv = __ddiv_rn(1.0, tm);
-      comx = __dmul_rn(wx, inv);
-      comy = __dmul_rn(wy, inv);
-      comz = __dmul_rn(wz, inv);
-    }
-    const double4 a = make_double4(comx, comy, comz, tm);
-    LevelNode rec;
-    rec.a = a;
-    rec.pre = pre;
-    rec.np = pe - pf;
-    rec.first = pf;
-    rec.leaf = leaf ? 1 : 0;
-    ws.lo_node[b] = rec;
-    // geometry
-    const unsigned long long key = ws.ukey[gf];
-    double cx = 0.0, cy = 0.0, cz = 0.0, h = 0.0;
-    if (level >= ws.sys_levels) {
-      const unsigned long long sys = key >> kSpatialBits;
-      if (sys >= (unsigned long long)ws.n_systems) {
-        record_error(sc, kStageGeometry, 2);
-        continue;
-      }
-      const double *box = ws.sys_box + 4 * (size_t)sys;
-      cx = box[0];
-      cy = box[1];
-      cz = box[2];
-      h = __dmul_rn(box[3], 0.5);
-      for (int d = ws.sys_levels + 1; d <= level; ++d) {
-        const int oct = (int)((key >> (kb - d * kDims)) & 7ull);
-        const double ch = __dmul_rn(h, 0.5);
-        cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
-        cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
-        cz = __dadd_rn(cz, (oct & 1) ? ch : -ch);
-        h = ch;
-      }
-      if (level == ws.sys_levels) ws.root_pre[sys] = pre;
-      if (!(h > 0.0)) record_error(sc, kStageTraversal, 8);
-    }
-    // traversal records
-    const double side = __dmul_rn(2.0, h);
-    const double ox = __dsub_rn(comx, cx), oy = __dsub_rn(comy, cy), oz = __dsub_rn(comz, cz);
-    const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
-    const double crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
-    const double c2 = __dmul_rn(crit, crit);
-    const double inner = __fma_rn(1.7320508075688774, h, __dsqrt_rn(o2));
-    const double cm = fmax(crit, inner) * (1.0 + 0x1p-40);
     for (int j = nk; j < 8; ++j) kids[j] = -1;
-    if (kRecords & kRecordsFp64) {
-      ws.node_a[pre] = a;
-      ws.node_b[pre] = make_double4(cx, cy, cz, h);
-      ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), cm * cm);
-      ws.node_meta[pre] = make_int4(skip, leaf ? pf : -1, leaf ? pe - pf : 0, nk);
-    }
-    if (kRecords & kRecordsMixed) {
-      MixedNode mrec;
-      mrec.a = a;
-      mrec.cr2 = __double2float_ru(cm * cm * (1.0 + 0x1p-18));
-      mrec.first = leaf ? pf : -1;
-      mrec.count = leaf ? pe - pf : 0;
-      mrec.nchild = nk;
-      ws.node_m[pre] = mrec;
-    }
+    const unsigned long long key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
+    if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key))
+      record_error(sc, kStageGeometry, 2);
   }
 }
 
@@ -1862,6 +1975,43 @@ __global__ void __launch_bounds__(kBlock) lo_group_mark_kernel(Workspace ws) {
       }
       run += cp;
     }
+  }
+}
+
+// The node-cache table: the cells of levels 0..kTopDepth with their mixed
+// records and child lists (read back from the step's records).
+__global__ void __launch_bounds__(128) lo_top_kernel(Workspace ws) {
+  __shared__ int s_base[kTopDepth + 3];
+  __shared__ int s_ok;
+  DevScalars *sc = ws.sc;
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int l = 0; l <= kTopDepth + 1; ++l) {
+      s_base[l] = run;
+      run += sc->level_count[l];
+    }
+    s_base[kTopDepth + 2] = run;
+    s_ok = !sc->error && sc->n_nodes > 0 && run <= sc->n_nodes;
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  const int count = min(s_base[kTopDepth + 1], kTopMax);
+  for (int q = threadIdx.x; q < count; q += blockDim.x) {
+    const int level = (q < s_base[1]) ? 0 : (q < s_base[2] ? 1 : 2);
+    const LevelNode nd = ws.lo_node[q];
+    const int c0 = ws.lo_first[q].y;
+    const int c1 = (q + 1 < s_base[level + 1]) ? ws.lo_first[q + 1].y : s_base[level + 2];
+    TopNode t;
+    t.rec = ws.node_m[nd.pre];
+    const int4 *k = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)nd.pre * 8);
+    const int4 k0 = k[0], k1 = k[1];
+    t.kids[0] = k0.x; t.kids[1] = k0.y; t.kids[2] = k0.z; t.kids[3] = k0.w;
+    t.kids[4] = k1.x; t.kids[5] = k1.y; t.kids[6] = k1.z; t.kids[7] = k1.w;
+    t.first_child = c0;
+    t.nchild = nd.leaf ? 0 : min(max(c1 - c0, 0), 8);
+    t.level = level;
+    t.pad = 0;
+    ws.top[q] = t;
   }
 }
 
@@ -2000,9 +2150,12 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part) {
     count_launches(1 + ws.sort_passes);
   }
   if (part != 1) {
-    // the first reader of the masses (gathered with the sorted positions)
-    groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, sorted, 1);
-    count_launches(1);
+    groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, sorted, 0);
+    // the first reader of the masses: the Morton-order gather, one particle
+    // per thread so that every thread's four loads are in flight at once
+    gather_sorted_kernel<<<(ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1, kBlock, 0, s>>>(
+        ws, ws.idx);
+    count_launches(2);
   }
   return cudaGetLastError();
 }
@@ -2043,8 +2196,14 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
   const int grid = grid_for(ws, 8);
   lo_span_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   lo_tile_scan_kernel<<<1, 32 * kLevelOrderChannels, 0, s>>>(ws);
-  lo_rank_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  for (int level = ws.max_level; level >= 0; --level) {
+  if (ws.records == kRecordsMixed)
+    lo_rank_kernel<kRecordsMixed><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
+  else if (ws.records == kRecordsFp64)
+    lo_rank_kernel<kRecordsFp64><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
+  else
+    lo_rank_kernel<kRecordsFp64 | kRecordsMixed><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
+  // the deepest level holds only leaves, which the rank pass finished
+  for (int level = ws.max_level - 1; level >= 0; --level) {
     if (ws.records == kRecordsMixed)
       lo_level_kernel<kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
     else if (ws.records == kRecordsFp64)
@@ -2052,9 +2211,13 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     else
       lo_level_kernel<kRecordsFp64 | kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
   }
+  if (ws.top && (ws.records & kRecordsMixed) && ws.n_systems == 1) {
+    lo_top_kernel<<<1, 128, 0, s>>>(ws);
+    count_launches(1);
+  }
   lo_group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(5 + (ws.max_level + 1));
+  count_launches(5 + ws.max_level);
   return cudaGetLastError();
 }
 

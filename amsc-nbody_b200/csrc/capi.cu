@@ -227,6 +227,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
     GET(ws.gspan, N);
     GET(ws.lo_first, C); GET(ws.lo_last, C); GET(ws.lo_node, C);
     GET(ws.lo_tiles, (size_t)ws.scan_tiles_n * kLevelOrderChannels);
+    GET(ws.top, (size_t)kTopMax);
   }
 #undef GET
   e = cudaMemset(ws.sc, 0, sizeof(DevScalars));
@@ -428,6 +429,7 @@ struct nbb_sim {
   cudaGraph_t step_graph_def = nullptr;
   uint64_t graph_kernels = 0;
   int tuned_group_size = 0;
+  int tuned_cache_depth = -1;     // mixed walk's node-cache depth; -1 untuned
   int tuned_fp64_grouping = -1;  // plain walk: 0 Morton slices, 1 octree groups; -1 untuned
   double min_softening = 0.0;  // ensembles: smallest per-system softening
   std::unique_ptr<RolloutRecord> rollout;
@@ -448,6 +450,7 @@ void nbb_config_default(nbb_config *cfg) {
   cfg->group_size = 0;
   cfg->use_graph = 1;
   cfg->device = 0;
+  cfg->cache_depth = -1;
 }
 
 int nbb_selftest_bounded_wait(void) {
@@ -495,6 +498,8 @@ static int validate_config(const nbb_config *c) {
     return fail(NBB_ERR_INVALID_ARGUMENT, "Unknown traversal precision");
   if (c->group_size != 0 && c->group_size != 32 && c->group_size != 64 && c->group_size != 128)
     return fail(NBB_ERR_INVALID_ARGUMENT, "group_size must be 0 (tuned), 32, 64 or 128");
+  if (c->cache_depth < -1 || c->cache_depth > kTopDepth)
+    return fail(NBB_ERR_INVALID_ARGUMENT, "cache_depth must be -1 (tuned), 0, 1 or 2");
   return NBB_OK;
 }
 
@@ -604,6 +609,9 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   tp.group_size = sim->cfg.group_size > 0 ? sim->cfg.group_size
                                           : (sim->tuned_group_size > 0 ? sim->tuned_group_size : 32);
   tp.group_mode = default_group_mode(tp.precision);
+  if (tp.precision == NBB_PRECISION_MIXED && sim->ws.top && sim->ws.n_systems == 1)
+    tp.cache_depth = sim->cfg.cache_depth >= 0 ? sim->cfg.cache_depth
+                                               : (sim->tuned_cache_depth > 0 ? sim->tuned_cache_depth : 0);
   if (tp.precision == NBB_PRECISION_FP64 && sim->tuned_fp64_grouping >= 0) tp.group_mode = sim->tuned_fp64_grouping;
   if (sim->ws.n_systems > 1) {
     tp.group_mode = 1;  // a warp's targets must share a system
@@ -612,62 +620,92 @@ static TraversalParams traversal_params(const nbb_sim *sim, int kick) {
   return tp;
 }
 
-// Group-size autotuner of the mixed walk: on the tree of the first force
-// evaluation, time the traversal (CUDA events, best of two) for each
-// candidate warp group size (32, 64 or 128 targets: 1, 2 or 4 per lane)
-// and keep the fastest.  The choice is cached per process for the particle
-// count's power-of-two bucket, so every simulation of that size in the
-// process uses the same size; pinning nbb_config.group_size skips tuning.
+// Autotuner of the mixed walk: on the tree of the first force evaluation,
+// time the traversal (CUDA events, best of three rounds) for each candidate warp group
+// size (32, 64 or 128 targets: 1, 2 or 4 per lane; only the configured one
+// when nbb_config.group_size pins it) and each node-cache depth (0, 1 or 2
+// levels below the root staged in shared memory; single systems), and keep
+// the fastest pair.  Results do not depend on the cache depth.  The choice is
+// cached per process for the particle count's power-of-two bucket and the
+// pinned group size, so every simulation of that size in the process uses
+// the same setting.
+struct MixedTuning {
+  int bucket, pinned, pinned_depth, group_size, cache_depth;
+};
 static std::mutex g_tune_lock;
-static std::vector<std::pair<int, int>> g_tuned;  // (log2 bucket, group size)
+static std::vector<MixedTuning> g_tuned;
 
-static int autotune_group_size(nbb_sim *sim) {
+static int autotune_mixed_walk(nbb_sim *sim) {
   Workspace &ws = sim->ws;
   int bucket = 0;
   while ((1 << bucket) < ws.n && bucket < 31) ++bucket;
+  const int pinned = sim->cfg.group_size;
+  bool found = false;
   {
     std::lock_guard<std::mutex> g(g_tune_lock);
-    for (const auto &kv : g_tuned)
-      if (kv.first == bucket) {
-        sim->tuned_group_size = kv.second;
+    for (const auto &t : g_tuned)
+      if (t.bucket == bucket && t.pinned == pinned && t.pinned_depth == sim->cfg.cache_depth) {
+        if (!pinned) sim->tuned_group_size = t.group_size;
+        sim->tuned_cache_depth = t.cache_depth;
+        found = true;
         break;
       }
   }
-  if (sim->tuned_group_size == 0) {
+  if (!found) {
     cudaStream_t s = sim->stream;
     cudaEvent_t e0, e1;
     NBB_CUDA(cudaEventCreate(&e0), "cudaEventCreate");
     NBB_CUDA(cudaEventCreate(&e1), "cudaEventCreate");
-    const int candidates[3] = {32, 64, 128};
-    float best = 1e30f;
-    int best_size = 32;
+    const int sizes[3] = {32, 64, 128};
+    const int n_sizes = pinned ? 1 : 3;
+    const int pinned_depth = sim->cfg.cache_depth;
+    const bool cacheable = ws.top && ws.n_systems == 1;
+    const int n_depths = (pinned_depth >= 0 || !cacheable) ? 1 : kTopDepth + 1;
+    // candidates timed round-robin (three rounds, best time of each) after
+    // one untimed walk, so that clock ramp-up and cache warm-up fall on no
+    // single candidate
+    float cand_ms[3][kTopDepth + 1];
+    for (auto &row : cand_ms)
+      for (float &v : row) v = 1e30f;
     cudaError_t e = cudaSuccess;
-    for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
-      TraversalParams tp = traversal_params(sim, 0);
-      tp.group_size = candidates[c];
-      ws.group_max = candidates[c];
-      for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
-        e = launch_retarget(ws, s);
-        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
-        if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
-        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
-        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-        float ms = 0.f;
-        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-        if (e == cudaSuccess && ms < best) {
-          best = ms;
-          best_size = candidates[c];
+    for (int round = -1; round < 3 && e == cudaSuccess; ++round) {
+      for (int c = 0; c < n_sizes && e == cudaSuccess; ++c) {
+        TraversalParams tp = traversal_params(sim, 0);
+        tp.group_size = pinned ? pinned : sizes[c];
+        ws.group_max = tp.group_size;
+        for (int d = 0; d < n_depths && e == cudaSuccess; ++d) {
+          tp.cache_depth = cacheable ? (pinned_depth >= 0 ? pinned_depth : d) : 0;
+          e = launch_retarget(ws, s);
+          if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+          if (e == cudaSuccess) e = launch_traversal(ws, tp, s);
+          if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+          if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+          float ms = 0.f;
+          if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+          if (e == cudaSuccess && round >= 0 && ms < cand_ms[c][d]) cand_ms[c][d] = ms;
+          if (round < 0) break;  // the warm-up walk: one candidate
         }
+        if (round < 0) break;
       }
     }
+    float best = 1e30f;
+    int best_size = pinned ? pinned : 32, best_depth = 0;
+    for (int c = 0; c < n_sizes; ++c)
+      for (int d = 0; d < n_depths; ++d)
+        if (cand_ms[c][d] < best) {
+          best = cand_ms[c][d];
+          best_size = pinned ? pinned : sizes[c];
+          best_depth = cacheable ? (pinned_depth >= 0 ? pinned_depth : d) : 0;
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (e != cudaSuccess) return cuda_fail(e, "group-size autotuning");
-    sim->tuned_group_size = best_size;
+    if (e != cudaSuccess) return cuda_fail(e, "mixed walk autotuning");
+    if (!pinned) sim->tuned_group_size = best_size;
+    sim->tuned_cache_depth = best_depth;
     std::lock_guard<std::mutex> g(g_tune_lock);
-    g_tuned.emplace_back(bucket, best_size);
+    g_tuned.push_back({bucket, pinned, sim->cfg.cache_depth, best_size, best_depth});
   }
-  // the initial acceleration comes from the chosen group size
+  // the initial acceleration comes from the chosen setting
   TraversalParams tp = traversal_params(sim, 0);
   ws.group_max = tp.group_size;
   NBB_CUDA(launch_retarget(ws, sim->stream), "retarget");
@@ -745,8 +783,8 @@ int nbb_sim_initialize(nbb_sim *sim) {
     sim->state = nbb_sim::State::failed;
     return st;
   }
-  if (sim->cfg.precision == NBB_PRECISION_MIXED && sim->cfg.group_size == 0) {
-    st = autotune_group_size(sim);
+  if (sim->cfg.precision == NBB_PRECISION_MIXED) {
+    st = autotune_mixed_walk(sim);
     if (st) {
       sim->state = nbb_sim::State::failed;
       return st;
@@ -1016,6 +1054,7 @@ int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats) {
   stats->mac_tests = (int64_t)sc.mac_tests;
   stats->group_size = sim->cfg.precision == NBB_PRECISION_MIXED ? traversal_params(sim, 0).group_size : 0;
   stats->stack_overflow = (int64_t)sc.stack_overflow;
+  stats->cache_depth = sim->cfg.precision == NBB_PRECISION_MIXED ? traversal_params(sim, 0).cache_depth : 0;
   return ok();
 }
 
@@ -1132,6 +1171,7 @@ int nbb_accel(size_t n, const double *mass, const double *x, const double *y, co
     stats->mac_tests = (int64_t)d.mac_tests;
     stats->group_size = precision == NBB_PRECISION_MIXED ? tp.group_size : 0;
     stats->stack_overflow = (int64_t)d.stack_overflow;
+    stats->cache_depth = 0;
   }
   if (export_out) {
     st = export_workspace(ws, export_out, sc.s, true);

@@ -109,6 +109,23 @@ struct __align__(16) LevelNode {
 };
 static_assert(sizeof(LevelNode) == 48, "two 32-byte sectors per node");
 
+// The top levels of the level-order octree (levels 0..kTopDepth: at most
+// 1 + 8 + 64 cells, in level order), the table the mixed walk's shared-memory
+// node cache is loaded from: each cell's record, its children's preorder
+// indices (visit order) and, for a cell whose children are cached too, their
+// place in the table (first child, count).
+constexpr int kTopDepth = 2;
+constexpr int kTopMax = 73;
+struct __align__(16) TopNode {
+  MixedNode rec;
+  int kids[8];
+  int first_child;  // level-order index of the first child
+  int nchild;
+  int level;
+  int pad;
+};
+static_assert(sizeof(TopNode) == 96, "record, child list, child range");
+
 // Per-tile counts of the level-order build (tiles of kScanTile groups): the
 // cells started per octree level, then the cells ended (kMaxLevels); the
 // rest pad a warp.
@@ -208,11 +225,12 @@ struct Workspace {
   // level-order build (simulation steps): the octree numbered level by level
   int level_order = 0;          // host: 1 when steps build the level-order octree
   int *gspan = nullptr;         // n: per group (delta + 1) | lambda << 8 | (delta_next + 1) << 16
-  int4 *lo_first = nullptr;     // cap: first group, first child, subtree end (preorder)
-  int2 *lo_last = nullptr;      // cap: last group, preorder index
+  int4 *lo_first = nullptr;     // cap: first particle, first child, subtree end (preorder), first group
+  int4 *lo_last = nullptr;      // cap: particle end, preorder index, key (low, high 32 bits)
   LevelNode *lo_node = nullptr;  // cap: mass, centre of mass, preorder index, particles
   int *lo_tiles = nullptr;      // scan_tiles_n * kLevelOrderChannels: per-tile counts, then their prefixes
   int records = kRecordsFp64 | kRecordsMixed;  // host: the records the level-order build writes
+  TopNode *top = nullptr;       // kTopMax: the top levels, for the mixed walk's node cache
   int *walk_ext = nullptr;    // walk_warps x walk_ext_cap: the mixed walk's stack below shared memory
 };
 
@@ -223,6 +241,14 @@ __device__ __forceinline__ void record_error(DevScalars *sc, int stage,
   atomicCAS(&sc->error, 0, stage * 100 + code);
 }
 
+// A relaxed load: for a word that carries its own flag and value (look-back
+// status), no ordering against other memory is needed, and several such
+// loads can be in flight at once.
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t *p) {
   uint32_t v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -288,6 +314,10 @@ struct TraversalParams {
   // warp target sets: 0 = fixed slices of 32 consecutive Morton-ordered
   // particles, 1 = octree target groups (contiguous, inside one parent cell)
   int group_mode = 0;
+  // mixed walk: tree levels below the root staged in shared memory per block
+  // (0: none; 1 or 2: the top 9 or 73 cells; level-order builds of a single
+  // system only)
+  int cache_depth = 0;
 };
 
 // Launch-count bookkeeping (kernels launched by this library).

@@ -296,6 +296,12 @@ __device__ __forceinline__ bool eval_batch(const PairList &list, const int *src,
   return singular;
 }
 
+// A child entry the mixed walk may push: a node's children come after it in
+// preorder; a cached cell's children are cached cells after it or any node.
+__device__ __forceinline__ bool valid_child(int kid, int node, int m, int mc) {
+  return node < m ? (kid > node && kid < m) : ((kid > node && kid < mc) || (kid >= 0 && kid < m));
+}
+
 // Per-lane target state of the mixed walk: negated target offsets from the
 // group centre, each duplicated into both halves of a pair.
 template <int kTPL>
@@ -413,6 +419,11 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
                                    kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : (kTPL == 2 ? NBB_MIXED_MINBLOCKS2 : NBB_MIXED_MINBLOCKS))
     traverse_mixed_kernel(Workspace ws, TraversalParams p) {
   __shared__ MixedShared<kTrackSource> sh;
+  // node cache: the top cache_depth levels below the root, loaded once per
+  // block from the step's table; stack entry m + q names cached cell q
+  __shared__ MixedNode c_rec[kTopMax];
+  __shared__ int4 c_kids[kTopMax][2];
+  __shared__ int s_ccount;
   DevScalars *sc = ws.sc;
   if (sc->error) return;
   const int lane = threadIdx.x & 31;
@@ -424,6 +435,31 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
   const int m = sc->n_nodes;
   const int n_groups = p.group_mode ? sc->n_tgroups : (n + 32 * kTPL - 1) / (32 * kTPL);
   const unsigned lt = lanemask_lt();
+  int ccount = 0;
+  if (p.cache_depth > 0 && ws.top && ws.n_systems == 1) {
+    if (threadIdx.x == 0) {
+      int cnt = 0;
+      for (int l = 0; l <= p.cache_depth && l <= kTopDepth; ++l) cnt += sc->level_count[l];
+      s_ccount = min(cnt, kTopMax);
+    }
+    __syncthreads();
+    ccount = s_ccount;
+    for (int q = threadIdx.x; q < ccount; q += blockDim.x) {
+      const TopNode &t = ws.top[q];
+      c_rec[q] = t.rec;
+      int kk[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        // children in visit order (descending level order); cached ones by slot
+        const int slot = t.first_child + t.nchild - 1 - j;
+        kk[j] = (t.level < p.cache_depth && j < t.nchild && slot < ccount) ? m + slot : t.kids[j];
+      }
+      c_kids[q][0] = make_int4(kk[0], kk[1], kk[2], kk[3]);
+      c_kids[q][1] = make_int4(kk[4], kk[5], kk[6], kk[7]);
+    }
+    __syncthreads();
+  }
+  const int mc = m + ccount;  // stack entries in [m, mc) are cached cells
   long long tests = 0;
   unsigned overflow = 0;
   long long inter_total = 0;
@@ -502,7 +538,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
     const float eps2f = (float)(soft * soft);
     const float2 eps2 = make_float2(eps2f, eps2f);
     int ls = 0;
-    if (lane == 0) stack[0] = root;
+    if (lane == 0) stack[0] = ccount > 0 ? m : root;
     int sp = (m > 0 && root >= 0 && root < m) ? 1 : 0;
     __syncwarp();
     // this warp's stack extension in global memory: when the shared part
@@ -546,14 +582,26 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       int4 k00 = make_int4(-1, -1, -1, -1), k01 = k00, k10 = k00, k11 = k00;
       double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
       float cr0 = 0.f, cr1 = 0.f;  // squared acceptance radius for a target box
-      if (n0 >= 0) {
+      if (n0 >= m) {
+        const MixedNode &rec = c_rec[n0 - m];
+        a0 = rec.a;
+        const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
+        cr0 = __int_as_float(meta.x);
+        m0 = make_int4(0, meta.y, meta.z, meta.w);
+      } else if (n0 >= 0) {
         const MixedNode &rec = ws.node_m[n0];
         a0 = rec.a;
         const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
         cr0 = __int_as_float(meta.x);
         m0 = make_int4(0, meta.y, meta.z, meta.w);
       }
-      if (n1 >= 0) {
+      if (n1 >= m) {
+        const MixedNode &rec = c_rec[n1 - m];
+        a1 = rec.a;
+        const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
+        cr1 = __int_as_float(meta.x);
+        m1 = make_int4(0, meta.y, meta.z, meta.w);
+      } else if (n1 >= 0) {
         const MixedNode &rec = ws.node_m[n1];
         a1 = rec.a;
         const int4 meta = *reinterpret_cast<const int4 *>(&rec.cr2);
@@ -593,14 +641,24 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       // child lists only of the nodes that open; their loads overlap the
       // prefix sums below
       if (nc0 > 0) {
-        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
-        k00 = kids[0];
-        if (nc0 > 4) k01 = kids[1];
+        if (n0 >= m) {
+          k00 = c_kids[n0 - m][0];
+          k01 = c_kids[n0 - m][1];
+        } else {
+          const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n0 * 8);
+          k00 = kids[0];
+          if (nc0 > 4) k01 = kids[1];
+        }
       }
       if (nc1 > 0) {
-        const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
-        k10 = kids[0];
-        if (nc1 > 4) k11 = kids[1];
+        if (n1 >= m) {
+          k10 = c_kids[n1 - m][0];
+          k11 = c_kids[n1 - m][1];
+        } else {
+          const int4 *kids = reinterpret_cast<const int4 *>(ws.node_kids + (size_t)n1 * 8);
+          k10 = kids[0];
+          if (nc1 > 4) k11 = kids[1];
+        }
       }
       int all_children;
       const int excl = warp_prefix_small<5>(nc0 + nc1, lt, all_children);
@@ -622,13 +680,13 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         const int kid[8] = {k00.x, k00.y, k00.z, k00.w, k01.x, k01.y, k01.z, k01.w};
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          if (j < nc0) stack[sp + excl + j] = (kid[j] > n0 && kid[j] < m) ? kid[j] : -1;
+          if (j < nc0) stack[sp + excl + j] = valid_child(kid[j], n0, m, mc) ? kid[j] : -1;
       }
       {
         const int kid[8] = {k10.x, k10.y, k10.z, k10.w, k11.x, k11.y, k11.z, k11.w};
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-          if (j < nc1) stack[sp + excl + nc0 + j] = (kid[j] > n1 && kid[j] < m) ? kid[j] : -1;
+          if (j < nc1) stack[sp + excl + nc0 + j] = valid_child(kid[j], n1, m, mc) ? kid[j] : -1;
       }
       sp += pushed;
       // accepted cells -> interaction list (fewer than 32 entries before,

@@ -34,7 +34,8 @@ PRECISION_MIXED = 1
 class Config(C.Structure):
     _fields_ = [("time_step", C.c_double), ("theta", C.c_double), ("softening", C.c_double),
                 ("gravitational_constant", C.c_double), ("precision", C.c_int),
-                ("group_size", C.c_int), ("use_graph", C.c_int), ("device", C.c_int)]
+                ("group_size", C.c_int), ("use_graph", C.c_int), ("device", C.c_int),
+                ("cache_depth", C.c_int)]
 
 
 class StateView(C.Structure):
@@ -44,7 +45,8 @@ class StateView(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("n_groups", C.c_int), ("n_octree_nodes", C.c_int), ("interactions", C.c_int64),
-                ("mac_tests", C.c_int64), ("group_size", C.c_int), ("stack_overflow", C.c_int64)]
+                ("mac_tests", C.c_int64), ("group_size", C.c_int), ("stack_overflow", C.c_int64),
+                ("cache_depth", C.c_int)]
 
 
 class TreeExport(C.Structure):

@@ -39,11 +39,12 @@ class SimulationConfig:
     group_size: int = 0
     use_graph: bool = True
     device: int = 0
+    cache_depth: int = -1  # mixed walk: tree levels staged in shared memory; -1 tuned
 
     def to_c(self) -> _lib.Config:
         return _lib.Config(self.time_step, self.theta, self.softening, self.gravitational_constant,
                            int(self.precision), int(self.group_size), int(bool(self.use_graph)),
-                           int(self.device))
+                           int(self.device), int(self.cache_depth))
 
 
 @dataclasses.dataclass

@@ -299,7 +299,7 @@ def run_nbb(args, rank, world, local):
                              "stages_ms": stage_ms, "interactions": st.interactions,
                              "mac_tests": st.mac_tests, "stack_overflow": st.stack_overflow,
                              "n_groups": st.n_groups, "n_octree_nodes": st.n_octree_nodes,
-                             "group_size": st.group_size}
+                             "group_size": st.group_size, "cache_depth": st.cache_depth}
         # end to end through the public API: pinned host state in, step, state out
         sim = sims["mixed"]
         pin = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in p.arrays()]
@@ -326,18 +326,17 @@ def run_nbb(args, rank, world, local):
     return p, results, e2e_ms, sampler.summary()
 
 
-# Algorithmic bytes of the rebuild (the minimum each stage must move), per
-# particle, per unique-key group, per radix node and per octree node: each
-# term is the sum of the arrays that stage must read once and write once.
+# Algorithmic bytes of the step's rebuild (the level-order build of a mixed
+# step): per particle, per unique-key group and per octree node, each term the
+# sum of the arrays that stage must read once and write once.
 BUILD_BYTES_PER_PARTICLE = 120 + 32 + 64 + 80 + 32  # KD+bbox, encode, 4 sort passes, groups+gather, leaf mass
-BUILD_BYTES_PER_GROUP = 12 + 28                     # group arrays, Karras internal node
-BUILD_BYTES_PER_RADIX_NODE = 20 + 40                # plan + scan, materialise
-BUILD_BYTES_PER_OCTREE_NODE = 108 + 78 + 100 + 224  # clear, geometry/child count, propagate, layout
+BUILD_BYTES_PER_GROUP = 24 + 20                     # level spans + counts, cell ranks (group payloads)
+BUILD_BYTES_PER_OCTREE_NODE = 32 + 208 + 112        # cell entries; level pass (entries, child records,
+                                                    # LevelNode, MixedNode, child list); target-group marks
 
 
 def build_algorithmic_bytes(n, groups, nodes):
-    return (BUILD_BYTES_PER_PARTICLE * n + BUILD_BYTES_PER_GROUP * groups
-            + BUILD_BYTES_PER_RADIX_NODE * (2 * groups - 1) + BUILD_BYTES_PER_OCTREE_NODE * nodes)
+    return BUILD_BYTES_PER_PARTICLE * n + BUILD_BYTES_PER_GROUP * groups + BUILD_BYTES_PER_OCTREE_NODE * nodes
 
 
 def load_peaks():
@@ -532,6 +531,7 @@ def bench_nbb(args, rank, world, local):
                               "algorithmic_bytes": build_bytes, "ms": build_ms,
                               "peak_source": hbm_source}
     line["group_size"] = mixed["group_size"]
+    line["cache_depth"] = mixed["cache_depth"]
     if rank == 0 and not args.no_error:
         rng = np.random.Generator(np.random.Philox(12345))
         tg = np.sort(rng.choice(args.n, min(ERROR_TARGETS, args.n), replace=False)).astype(np.int32)

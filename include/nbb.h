@@ -63,6 +63,8 @@ typedef struct {
   int group_size; /* MIXED: targets per warp group, 32/64/128; 0 = tuned */
   int use_graph;  /* capture each step into a CUDA graph (default 1) */
   int device;     /* CUDA device ordinal (default 0) */
+  int cache_depth; /* MIXED: tree levels below the root staged in shared memory
+                      per block: -1 = tuned (default), 0, 1 or 2 */
 } nbb_config;
 
 /* Defaults of BarnesHutParameters (theta 0.5, softening 1e-6, G = SI);
@@ -163,6 +165,8 @@ typedef struct {
   int64_t stack_overflow; /* MIXED: nodes accepted because the walk's stack was
                              full (their children would not fit); 0 in a walk
                              that applied the acceptance test everywhere */
+  int cache_depth;      /* MIXED: tree levels below the root the walk stages in
+                           shared memory per block (0, 1 or 2; autotuned) */
 } nbb_stats;
 int nbb_sim_stats(nbb_sim *sim, nbb_stats *stats);
 

@@ -115,3 +115,35 @@ def test_level_order_build_on_an_ensemble(nbb_mod):
         soft = 0.02 if ens.softening is None else float(ens.softening[k])
         ref = np.stack(nbb_mod.compute_accelerations(part, 0.5, soft, 1.0))
         assert np.array_equal(acc[:, sl], ref), k
+
+
+@pytest.mark.parametrize("case,group_size", [("plummer", 64), ("disk", 32), ("blobs", 128)])
+def test_node_cache_depth_changes_no_result(nbb_mod, case, group_size):
+    """The mixed walk's shared-memory node cache (the top 0, 1 or 2 levels
+    below the root, loaded per block from the step's table) relocates records
+    only: accelerations and walk counts equal the uncached walk's."""
+    p = _case(case)
+    outs = []
+    for depth in (0, 1, 2):
+        sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=nbb_mod.PRECISION_MIXED,
+                                                             group_size=group_size, cache_depth=depth))
+        sim.initialize()
+        sim.run(2)
+        st = sim.stats()
+        assert st.cache_depth == depth and st.stack_overflow == 0
+        outs.append((sim.download() + sim.accelerations(), st.interactions, st.mac_tests))
+    for got, inter, tests in outs[1:]:
+        assert inter == outs[0][1] and tests == outs[0][2]
+        for a, b in zip(got, outs[0][0]):
+            assert np.array_equal(a, b)
+
+
+def test_node_cache_depth_tuned_and_validated(nbb_mod):
+    p = _case("plummer")
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=nbb_mod.PRECISION_MIXED))
+    sim.initialize()
+    assert sim.stats().cache_depth in (0, 1, 2)
+    for bad in (-2, 3):
+        with pytest.raises(nbb_mod.InvalidArgument):
+            nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=nbb_mod.PRECISION_MIXED,
+                                                           cache_depth=bad))
