@@ -540,10 +540,15 @@ cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const 
   const int grid = grid_of_ws(ws, 8);
   adj_reset_kernel<<<1, 32, 0, s>>>(ws.sc);
   adj_topology_kernel<<<grid, kBlock, 0, s>>>(ws, ab.pparent, ab.prange, nullptr);
-  adjoint_walk_kernel<<<grid_of_ws(ws, 8), 256, 0, s>>>(ws, p, ab);
+  if (p.precision == 1) {
+    e = launch_adjoint_mixed(ws, p, ab, s);
+    if (e != cudaSuccess) return e;
+  } else {
+    adjoint_walk_kernel<<<grid_of_ws(ws, 8), 256, 0, s>>>(ws, p, ab);
+  }
   adj_node_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
   adj_leaf_kernel<<<grid, kBlock, 0, s>>>(ws, ab);
-  count_launches(5);
+  count_launches(p.precision == 1 ? 4 : 5);
   return cudaGetLastError();
 }
 

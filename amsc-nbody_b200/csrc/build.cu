@@ -1665,9 +1665,8 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
 // tile prefixes) plus the ranks inside the tile.  Writes each cell's first
 // particle, first child, subtree end and first group (by its first group) and
 // its particle end, preorder index and key (by its last group; every group of
-// a cell carries the cell's prefix).  A group's leaf (level lambda, preorder
-// index S(g) - 1) is finished here: mass and centre of mass of its particles
-// in sorted order (octree_physics.cu:95-154) and its records.
+// a cell carries the cell's prefix), and per group its leaf's level-order
+// index and S(g) (the leaf sits at level lambda, preorder index S(g) - 1).
 template <int kRecords>
 __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, double theta) {
   constexpr int kWarps = kScanThreads / 32;
@@ -1828,9 +1827,49 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
           record_error(sc, kStageLayout, 1);
       }
     }
-    // the leaf: its particles in sorted order, its records at S(g) - 1
-    const int pre = s_from - 1;
-    if (bleaf < 0 || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n) {
+    // the leaf (level lambda, preorder index S(g) - 1), finished by lo_leaf_kernel
+    if (bleaf < 0 || s_from < 1 || s_from > M) {
+      record_error(sc, kStageLayout, 1);
+      continue;
+    }
+    ws.lo_gleaf[g] = make_int2(bleaf, s_from);
+  }
+}
+
+// The target-group rule (group_mark_kernel) for one cell of the level-order
+// octree: whether the cell is one group by itself (then it marks its first
+// particle only as a whole system); otherwise an occupied leaf marks slices
+// of group_max and any other cell the starts of its children's runs
+// (children in octant order, packed greedily when the cell is compact).
+__device__ __forceinline__ bool lo_whole_group(const Workspace &ws, int level, int np, bool leaf) {
+  const bool virt = level < ws.sys_levels;  // children are other systems
+  const bool compact = !virt && (leaf || np <= 1 || level - ws.sys_levels >= ws.group_depth);
+  return !virt && np <= ws.group_max && compact;
+}
+
+// Occupied leaves, one group per thread: mass and centre of mass of the
+// group's particles in sorted order (octree_physics.cu:95-154), the leaf's
+// records at preorder index S(g) - 1 (no child list: neither walk reads one
+// for an occupied leaf), and its target-group marks.
+template <int kRecords>
+__global__ void __launch_bounds__(kBlock) lo_leaf_kernel(Workspace ws, double theta) {
+  __shared__ int s_g, s_m;
+  DevScalars *sc = ws.sc;
+  if (threadIdx.x == 0) {
+    const int g = sc->n_groups, m = sc->n_nodes;
+    s_g = (!sc->error && g > 0 && g <= ws.n && m > 0) ? g : 0;
+    s_m = m;
+  }
+  __syncthreads();
+  const int G = s_g, M = s_m;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    const int2 lf = ws.lo_gleaf[g];
+    const int pf = ws.gfirst[g], pe = ws.glast[g] + 1;
+    const unsigned long long key = ws.ukey[g];
+    const int lam = (ws.gspan[g] >> 8) & 255;
+    const int bleaf = lf.x, skip = lf.y, pre = skip - 1;
+    if (bleaf < 0 || bleaf >= M || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n ||
+        lam < 1 || lam > ws.max_level) {
       record_error(sc, kStageLayout, 1);
       continue;
     }
@@ -1842,11 +1881,14 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
       wy = __fma_rn(q.w, q.y, wy);
       wz = __fma_rn(q.w, q.z, wz);
     }
-    int4 *kids = reinterpret_cast<int4 *>(ws.node_kids + (size_t)pre * 8);
-    kids[0] = make_int4(-1, -1, -1, -1);
-    kids[1] = make_int4(-1, -1, -1, -1);
-    if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, s_from, pf, pe, true, 0, tm, wx, wy, wz, key))
+    if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, skip, pf, pe, true, 0, tm, wx, wy, wz, key))
       record_error(sc, kStageGeometry, 2);
+    const int np = pe - pf;
+    if (lo_whole_group(ws, lam, np, true)) {
+      if (lam == ws.sys_levels) ws.tflag[pf] = 1;
+    } else {
+      for (int k = 0; k < np; k += ws.group_max) ws.tflag[pf + k] = 1;
+    }
   }
 }
 
@@ -1895,6 +1937,15 @@ __global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int l
     const int nk = c1 - c0;
     // children in visit order: octant 7 -> 0, the children in descending key order
     int *kids = ws.node_kids + (size_t)pre * 8;
+    // target groups (group_mark_kernel's rule): a whole system that is one
+    // group, else the starts of the children's runs
+    const int np = pe - pf;
+    const bool whole = lo_whole_group(ws, level, np, false);
+    if (whole && level == ws.sys_levels) ws.tflag[pf] = 1;
+    const bool virt = level < ws.sys_levels;
+    const bool merge = !virt && (np <= 1 || level - ws.sys_levels >= ws.group_depth);
+    const bool child_compact_level = level + 1 - ws.sys_levels >= ws.group_depth;
+    int run = 0;
     double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -1906,6 +1957,19 @@ __global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int l
         wy = __fma_rn(cm, ch.a.y, wy);
         wz = __fma_rn(cm, ch.a.z, wz);
         kids[nk - 1 - j] = ch.pre;
+        if (!whole) {
+          if (virt) run = 0;
+          const int cp = ch.np;
+          if (cp > ws.group_max || !(ch.leaf || cp <= 1 || child_compact_level)) {
+            run = 0;  // the child splits itself
+          } else {
+            if (!merge || run == 0 || run + cp > ws.group_max) {
+              if (ch.first >= 0 && ch.first < ws.n) ws.tflag[ch.first] = 1;
+              run = 0;
+            }
+            run += cp;
+          }
+        }
       }
     }
     for (int j = nk; j < 8; ++j) kids[j] = -1;
@@ -2193,7 +2257,6 @@ cudaError_t launch_tree(Workspace &ws, double theta, cudaStream_t s) {
 
 cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s) {
   if (!ws.lo_tiles) return cudaErrorInvalidValue;
-  const int grid = grid_for(ws, 8);
   lo_span_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   lo_tile_scan_kernel<<<1, 32 * kLevelOrderChannels, 0, s>>>(ws);
   if (ws.records == kRecordsMixed)
@@ -2202,7 +2265,14 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     lo_rank_kernel<kRecordsFp64><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
   else
     lo_rank_kernel<kRecordsFp64 | kRecordsMixed><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
-  // the deepest level holds only leaves, which the rank pass finished
+  const int leaf_grid = (ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1;
+  if (ws.records == kRecordsMixed)
+    lo_leaf_kernel<kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+  else if (ws.records == kRecordsFp64)
+    lo_leaf_kernel<kRecordsFp64><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+  else
+    lo_leaf_kernel<kRecordsFp64 | kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+  // the deepest level holds only leaves
   for (int level = ws.max_level - 1; level >= 0; --level) {
     if (ws.records == kRecordsMixed)
       lo_level_kernel<kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
@@ -2215,7 +2285,7 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     lo_top_kernel<<<1, 128, 0, s>>>(ws);
     count_launches(1);
   }
-  lo_group_mark_kernel<<<grid, kBlock, 0, s>>>(ws);
+  // target-group marks were set by the leaf and level passes
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
   count_launches(5 + ws.max_level);
   return cudaGetLastError();

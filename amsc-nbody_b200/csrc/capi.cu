@@ -225,7 +225,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   if (level_order) {
     ws.level_order = 1;
     GET(ws.gspan, N);
-    GET(ws.lo_first, C); GET(ws.lo_last, C); GET(ws.lo_node, C);
+    GET(ws.lo_first, C); GET(ws.lo_last, C); GET(ws.lo_node, C); GET(ws.lo_gleaf, N);
     GET(ws.lo_tiles, (size_t)ws.scan_tiles_n * kLevelOrderChannels);
     GET(ws.top, (size_t)kTopMax);
   }
@@ -1819,10 +1819,14 @@ int nbb_sim_backward(nbb_sim *sim, const double *gx, const double *gy, const dou
   ab.tgt_g = rec.tgt_g;
   ab.pparent = rec.pparent;
   ab.prange = rec.prange;
+  // the VJP of the force the rollout ran: the plain form's, or the mixed
+  // form's on its own interaction lists (32-target groups)
   TraversalParams tpa = traversal_params(sim, 0);
-  tpa.precision = 0;
+  tpa.precision = sim->cfg.precision == NBB_PRECISION_MIXED ? 1 : 0;
   tpa.kick = 0;
-  tpa.group_mode = 1;  // compact warps; the sums per interaction do not depend on it
+  tpa.group_mode = 1;  // compact warps; the plain form's sums do not depend on it
+  tpa.group_size = 32;
+  tpa.cache_depth = 0;
   cudaError_t e = cudaSuccess;
   if (S > 0) {
     // the step s -> s+1 is undone by the VJP at x_{s+1} with accelerations

@@ -143,6 +143,7 @@ struct Workspace {
   int num_sms = 0;
   int fp64_grid = 0;    // persistent traversal grids (blocks)
   int mixed_grid[2][3] = {{0, 0, 0}, {0, 0, 0}};  // [track source][1, 2 or 4 targets per lane]
+  int vjp_grid = 0;     // the mixed walk's adjoint form
   int walk_warps = 0;     // warps of the largest mixed-walk grid
   int walk_ext_cap = 0;   // entries per warp of the mixed walk's stack extension
   int group_max = 32;   // largest octree target group: 32, 64 or 128 (32 x target slots per lane)
@@ -227,6 +228,7 @@ struct Workspace {
   int *gspan = nullptr;         // n: per group (delta + 1) | lambda << 8 | (delta_next + 1) << 16
   int4 *lo_first = nullptr;     // cap: first particle, first child, subtree end (preorder), first group
   int4 *lo_last = nullptr;      // cap: particle end, preorder index, key (low, high 32 bits)
+  int2 *lo_gleaf = nullptr;     // n: per group, its leaf's level-order index and S(g)
   LevelNode *lo_node = nullptr;  // cap: mass, centre of mass, preorder index, particles
   int *lo_tiles = nullptr;      // scan_tiles_n * kLevelOrderChannels: per-tile counts, then their prefixes
   int records = kRecordsFp64 | kRecordsMixed;  // host: the records the level-order build writes
@@ -473,9 +475,14 @@ cudaError_t launch_potential_tree(Workspace &ws, const TraversalParams &p, doubl
 cudaError_t launch_potential_direct(const double *m, const double *x, const double *y, const double *z, int n,
                                     double g, double soft, double *phi, cudaStream_t s);
 
-// VJP of the plain FP64 force on the current tree (built from the positions
-// in the workspace): accumulates into ab.gx / gy / gz / gm.
+// VJP of the force on the current tree (built from the positions in the
+// workspace): the plain FP64 form's (p.precision 0) or the mixed form's (1,
+// on the mixed walk's interaction lists); accumulates into ab.gx / gy / gz / gm.
 cudaError_t launch_adjoint_force(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,
+                                 cudaStream_t s);
+// The mixed walk evaluating the VJP (node / particle / target cotangents into
+// ab.node_g, ab.part_g, ab.tgt_g).
+cudaError_t launch_adjoint_mixed(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,
                                  cudaStream_t s);
 // Forces on every perturbed copy with the current tree's structure
 // (accelerations into fb.ax / ay / az).

@@ -333,14 +333,121 @@ __device__ __forceinline__ bool eval_slots(const PairList &list, const int *src,
   return eval_batch<kTrackSource, 1, eval_unroll<kTPL>()>(list, src, count, t.s, t.ntx, t.nty, t.ntz, eps2, t.sum, t.comp);
 }
 
-template <bool kTrackSource, int kTPL>
+// ------------------------------------------------- mixed adjoint walk ----
+//
+// Vector-Jacobian product of the mixed form's force, on the mixed walk's own
+// interaction lists (group-box acceptance, FP32 offsets from the group
+// centre).  For target i, entry s (mass mu, offset r = Y_s - x_i) and the
+// accelerations cotangent c_i (see adjoint.cu's file comment):
+//   u = G mu (inv3 c_i - 3 inv5 (r . c_i) r),  d/dx_i -= u,  d/dY_s += u,
+//   d/dmu_s += G inv3 (r . c_i),
+// in FP32 with the hardware reciprocal square root.  A source's u is summed
+// over the warp's targets before it is added (FP64 atomics) to the cell's or
+// particle's cotangent; the list names each entry's source: a particle by its
+// Morton slot, a cell by -3 - its preorder index.
+
+// Cotangent state of the adjoint walk's target (one per lane).
+struct LaneVjp {
+  float cx = 0.f, cy = 0.f, cz = 0.f;  // accelerations cotangent
+  double gx = 0.0, gy = 0.0, gz = 0.0;  // position cotangent (running)
+};
+
+// Sum over the warp of 8 per-lane values, transposed: lane l ends with the
+// total of value ((l >> 4) & 1) * 4 + ((l >> 3) & 1) * 2 + ((l >> 2) & 1)
+// (the four lanes of a quad hold the same total) -- 9 shuffles for 8 sums.
+__device__ __forceinline__ float warp_sum8_transposed(float (&v)[8], int lane) {
+  const bool u16 = lane & 16, u8 = lane & 8, u4 = lane & 4;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float send = u16 ? v[i] : v[i + 4];
+    const float keep = u16 ? v[i + 4] : v[i];
+    v[i] = keep + __shfl_xor_sync(kFull, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float send = u8 ? v[i] : v[i + 2];
+    const float keep = u8 ? v[i + 2] : v[i];
+    v[i] = keep + __shfl_xor_sync(kFull, send, 8);
+  }
+  const float send = u4 ? v[0] : v[1];
+  float x = (u4 ? v[1] : v[0]) + __shfl_xor_sync(kFull, send, 4);
+  x += __shfl_xor_sync(kFull, x, 2);
+  x += __shfl_xor_sync(kFull, x, 1);
+  return x;
+}
+
+// VJP of `count` list entries (zero-mass pads contribute nothing) for the
+// lane's target; returns true on a singular pair.
+__device__ bool vjp_entries(const PairList &list, const int *src, int count, int self, bool valid, float ntx,
+                            float nty, float ntz, LaneVjp &v, float eps2, float g, const AdjointBuffers &ab) {
+  const int lane = threadIdx.x & 31;
+  bool singular = false;
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  for (int e0 = 0; e0 < count; e0 += 8) {
+    float ux[8], uy[8], uz[8], uw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      ux[k] = uy[k] = uz[k] = uw[k] = 0.f;
+      const int e = e0 + k;
+      if (e >= count) continue;  // warp-uniform
+      const float4 ea = list.a[e >> 1], eb = list.b[e >> 1];
+      const bool hi = e & 1;
+      const float ex = hi ? ea.y : ea.x, ey = hi ? ea.w : ea.z, ez = hi ? eb.y : eb.x, mu = hi ? eb.w : eb.z;
+      const float dx = ex + ntx, dy = ey + nty, dz = ez + ntz;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+      if (!valid || src[e] == self || mu == 0.f) continue;
+      if (!(r2 > 0.f)) {
+        singular = true;
+        continue;
+      }
+      const float r = rsqrt_approx(r2);
+      const float rr = r * r;
+      const float gi3 = g * rr * r;
+      const float rc = fmaf(dx, v.cx, fmaf(dy, v.cy, dz * v.cz));
+      const float f = gi3 * mu;
+      const float h = 3.f * f * rr * rc;
+      ux[k] = fmaf(f, v.cx, -h * dx);
+      uy[k] = fmaf(f, v.cy, -h * dy);
+      uz[k] = fmaf(f, v.cz, -h * dz);
+      uw[k] = gi3 * rc;
+      gx -= ux[k];
+      gy -= uy[k];
+      gz -= uz[k];
+    }
+    const float sx = warp_sum8_transposed(ux, lane);
+    const float sy = warp_sum8_transposed(uy, lane);
+    const float sz = warp_sum8_transposed(uz, lane);
+    const float sw = warp_sum8_transposed(uw, lane);
+    const int e = e0 + ((((lane >> 4) & 1) << 2) | (((lane >> 3) & 1) << 1) | ((lane >> 2) & 1));
+    const int comp = lane & 3;
+    const float val = comp == 0 ? sx : (comp == 1 ? sy : (comp == 2 ? sz : sw));
+    if (e < count && val != 0.f) {
+      const int sr = src[e];
+      double *dst = nullptr;
+      if (sr >= 0) dst = reinterpret_cast<double *>(ab.part_g + sr);
+      else if (sr <= -3) dst = reinterpret_cast<double *>(ab.node_g + (-3 - sr));
+      if (dst) atomicAdd(dst + comp, (double)val);
+    }
+  }
+  v.gx += gx;
+  v.gy += gy;
+  v.gz += gz;
+  return singular;
+}
+
+template <bool kTrackSource, int kTPL, bool kVjp>
 __device__ __forceinline__ void flush_full(const PairList &list, int *src, int &ls, LaneTargets<kTPL> &lt_,
-                                           float2 eps2, int nq) {
+                                           LaneVjp &vj, float2 eps2, int nq, float g, const AdjointBuffers &ab) {
   const int lane = threadIdx.x & 31;
   int done = 0;
   while (ls - done >= 32) {
     const PairList part{list.a + done / 2, list.b + done / 2};
-    const bool sg = eval_slots<kTrackSource, kTPL>(part, src + (kTrackSource ? done : 0), 32, nq, lt_, eps2);
+    bool sg;
+    if constexpr (kVjp)
+      sg = vjp_entries(part, src + done, 32, lt_.s[0], lt_.valid[0], lt_.ntx[0].x, lt_.nty[0].x, lt_.ntz[0].x, vj,
+                       eps2.x, g, ab);
+    else
+      sg = eval_slots<kTrackSource, kTPL>(part, src + (kTrackSource ? done : 0), 32, nq, lt_, eps2);
 #pragma unroll
     for (int q = 0; q < kTPL; ++q)
       if (lt_.valid[q]) {
@@ -414,10 +521,13 @@ __device__ __forceinline__ bool accept_box(const double4 &a, const double *gbox,
 // gets the acceptance test.  Accepted nodes and the particles of reached leaves go to
 // a shared interaction list as FP32 offsets from the group centre (formed in
 // FP64, then rounded) and are evaluated by all lanes in batches of 32.
-template <bool kTrackSource, int kTPL>
+// With kVjp (one target per lane, sources tracked) the same walk evaluates
+// the vector-Jacobian product above instead of the force.
+template <bool kTrackSource, int kTPL, bool kVjp = false>
 __global__ void __launch_bounds__(kMixedWarps * 32,
                                    kTPL >= 4 ? NBB_MIXED_MINBLOCKS4 : (kTPL == 2 ? NBB_MIXED_MINBLOCKS2 : NBB_MIXED_MINBLOCKS))
-    traverse_mixed_kernel(Workspace ws, TraversalParams p) {
+    traverse_mixed_kernel(Workspace ws, TraversalParams p, AdjointBuffers ab) {
+  static_assert(!kVjp || (kTrackSource && kTPL == 1), "the adjoint walk tracks sources, one target per lane");
   __shared__ MixedShared<kTrackSource> sh;
   // node cache: the top cache_depth levels below the root, loaded once per
   // block from the step's table; stack entry m + q names cached cell q
@@ -473,6 +583,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
     const int g1 = p.group_mode ? ((grp + 1 < n_groups) ? ws.tstart[grp + 1] : n) : min(g0 + 32 * kTPL, n);
     const int nq = min(kTPL, max(1, (g1 - g0 + 31) >> 5));  // occupied target slots
     LaneTargets<kTPL> T;
+    LaneVjp V;
     double4 tp[kTPL];
     double lo[3], hi[3];
 #pragma unroll
@@ -482,6 +593,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       tp[q] = ws.pm4[T.valid[q] ? T.s[q] : g0];
       T.sum[q] = make_float3(0.f, 0.f, 0.f);
       T.comp[q] = make_float3(0.f, 0.f, 0.f);
+    }
+    if (kVjp && T.valid[0]) {
+      const uint32_t ti = ws.idx[T.s[0]];
+      V.cx = (float)(ab.coef * ab.gvx[ti]);
+      V.cy = (float)(ab.coef * ab.gvy[ti]);
+      V.cz = (float)(ab.coef * ab.gvz[ti]);
     }
     lo[0] = hi[0] = tp[0].x;
     lo[1] = hi[1] = tp[0].y;
@@ -696,12 +813,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
       if (cat0 == 1) {
         const int pos = ls + __popc(cm0 & lt);
         list.put(pos, e0.x, e0.y, e0.z, e0.w);
-        if (kTrackSource) src[pos] = -1;
+        if (kTrackSource) src[pos] = kVjp ? -3 - n0 : -1;
       }
       if (cat1 == 1) {
         const int pos = ls + __popc(cm0) + __popc(cm1 & lt);
         list.put(pos, e1.x, e1.y, e1.z, e1.w);
-        if (kTrackSource) src[pos] = -1;
+        if (kTrackSource) src[pos] = kVjp ? -3 - n1 : -1;
       }
       ls += __popc(cm0) + __popc(cm1);
       // reached leaves -> their particles: all at once when they fit
@@ -746,12 +863,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         }
         ls += ltotal;
         __syncwarp();
-        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
+        flush_full<kTrackSource, kTPL, kVjp>(list, src, ls, T, V, eps2, nq, (float)p.g, ab);
       } else {
         // rare: the leaves' particles do not fit behind the list; their
         // ranges stay in registers through the flush
         __syncwarp();
-        flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
+        flush_full<kTrackSource, kTPL, kVjp>(list, src, ls, T, V, eps2, nq, (float)p.g, ab);
         for (int h = 0; h < 2; ++h) {
           unsigned lm = __ballot_sync(kFull, (h == 0 ? lc0 : lc1) > 0);
           while (lm) {
@@ -769,7 +886,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
               }
               ls += (cnt - b0 < 32) ? (cnt - b0) : 32;
               __syncwarp();
-              flush_full<kTrackSource, kTPL>(list, src, ls, T, eps2, nq);
+              flush_full<kTrackSource, kTPL, kVjp>(list, src, ls, T, V, eps2, nq, (float)p.g, ab);
             }
           }
         }
@@ -785,7 +902,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         }
         __syncwarp();
       }
-      const bool sg = eval_slots<kTrackSource, kTPL>(list, src, ls, nq, T, eps2);
+      bool sg;
+      if constexpr (kVjp)
+        sg = vjp_entries(list, src, ls + (ls & 1), T.s[0], T.valid[0], T.ntx[0].x, T.nty[0].x, T.ntz[0].x, V, eps2.x,
+                         (float)p.g, ab);
+      else
+        sg = eval_slots<kTrackSource, kTPL>(list, src, ls, nq, T, eps2);
 #pragma unroll
       for (int q = 0; q < kTPL; ++q)
         if (T.valid[q]) {
@@ -794,9 +916,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         }
     }
     __syncwarp();
+    if constexpr (kVjp) {
+      if (T.valid[0]) ab.tgt_g[T.s[0]] = make_double4(V.gx, V.gy, V.gz, 0.0);
+    }
 #pragma unroll
     for (int q = 0; q < kTPL; ++q) {
-      if (!T.valid[q]) continue;
+      if (kVjp || !T.valid[q]) continue;
       const double ax = p.g * ((double)T.sum[q].x - (double)T.comp[q].x);
       const double ay = p.g * ((double)T.sum[q].y - (double)T.comp[q].y);
       const double az = p.g * ((double)T.sum[q].z - (double)T.comp[q].z);
@@ -1146,6 +1271,7 @@ cudaError_t configure_traversal(Workspace &ws) {
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 2>, kMixedWarps * 32, sms, ws.mixed_grid[1][1]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<false, 4>, kMixedWarps * 32, sms, ws.mixed_grid[0][2]);
   if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 4>, kMixedWarps * 32, sms, ws.mixed_grid[1][2]);
+  if (e == cudaSuccess) e = grid_of(traverse_mixed_kernel<true, 1, true>, kMixedWarps * 32, sms, ws.vjp_grid);
   // The stack extension holds a whole walk: the stack stays sorted by tree
   // level (a round pops the top and pushes children one level deeper), and
   // a level's entries are pushed only after every older entry of that level
@@ -1168,11 +1294,26 @@ cudaError_t launch_traversal(Workspace &ws, const TraversalParams &p, cudaStream
   if (p.precision == 0)
     traverse_fp64_kernel<<<ws.fp64_grid > 0 ? ws.fp64_grid : 148, 256, 0, s>>>(ws, p);
   else if (slot == 0)
-    (track ? traverse_mixed_kernel<true, 1> : traverse_mixed_kernel<false, 1>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+    (track ? traverse_mixed_kernel<true, 1> : traverse_mixed_kernel<false, 1>)<<<grid, kMixedWarps * 32, 0, s>>>(
+        ws, p, AdjointBuffers{});
   else if (slot == 1)
-    (track ? traverse_mixed_kernel<true, 2> : traverse_mixed_kernel<false, 2>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+    (track ? traverse_mixed_kernel<true, 2> : traverse_mixed_kernel<false, 2>)<<<grid, kMixedWarps * 32, 0, s>>>(
+        ws, p, AdjointBuffers{});
   else
-    (track ? traverse_mixed_kernel<true, 4> : traverse_mixed_kernel<false, 4>)<<<grid, kMixedWarps * 32, 0, s>>>(ws, p);
+    (track ? traverse_mixed_kernel<true, 4> : traverse_mixed_kernel<false, 4>)<<<grid, kMixedWarps * 32, 0, s>>>(
+        ws, p, AdjointBuffers{});
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_mixed(Workspace &ws, const TraversalParams &p, const AdjointBuffers &ab,
+                                 cudaStream_t s) {
+  // the stack extension is sized for the largest mixed grid
+  int grid = ws.vjp_grid > 0 ? ws.vjp_grid : 148;
+  if (ws.walk_warps > 0 && grid * kMixedWarps > ws.walk_warps) grid = ws.walk_warps / kMixedWarps;
+  TraversalParams q = p;
+  q.cache_depth = 0;  // cached cells carry no preorder index
+  traverse_mixed_kernel<true, 1, true><<<grid, kMixedWarps * 32, 0, s>>>(ws, q, ab);
   count_launches(1);
   return cudaGetLastError();
 }

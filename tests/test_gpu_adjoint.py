@@ -172,10 +172,28 @@ def test_backward_restores_state_and_is_repeatable(nbb_mod, precision):
     assert np.array_equal(np.stack(sim.download()), np.stack(ref.download()))
 
 
+def test_mixed_theta_zero_adjoint_equals_direct_sum_adjoint(nbb_mod):
+    """The mixed form's VJP (FP32, on the mixed walk's lists) at theta = 0,
+    where the walk opens every cell: the exact all-pairs adjoint up to FP32
+    rounding."""
+    n = 1024
+    p = _plummer(nbb_mod, n, 9)
+    wx, wv = _linear_loss_weights(n, 10)
+    sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.0, 0.01, 1.0, precision=nbb_mod.PRECISION_MIXED))
+    sim.initialize()
+    sim.rollout(12, 5)
+    gm, gx, gv = sim.backward(wx, wv)
+    _, dm, dx, dv = nbb_mod.direct_rollout_adjoint(p, nbb_mod.SimulationConfig(1e-3, 0.0, 0.01, 1.0), 12, wx, wv)
+    for a, b in ((gm, dm), (gx, dx), (gv, dv)):
+        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(b)
+
+
 @pytest.mark.parametrize("group_size", [0, 32, 64, 128])
 def test_mixed_rollout_gradient_close_to_fp64_gradient(nbb_mod, group_size):
-    # the backward pass rebuilds one-warp target groups whatever group size
-    # the mixed walk uses
+    # the mixed rollout is differentiated with the mixed force's own VJP
+    # (group-box acceptance, FP32): its gradient differs from the plain
+    # form's at the level of the mixed form's force error; the backward pass
+    # rebuilds one-warp target groups whatever group size the walk uses
     n = 4096
     p = _plummer(nbb_mod, n, 19)
     wx, wv = _linear_loss_weights(n, 20)
@@ -187,7 +205,7 @@ def test_mixed_rollout_gradient_close_to_fp64_gradient(nbb_mod, group_size):
         sim.rollout(12, 4)
         out.append(sim.backward(wx, wv))
     for a, b in zip(out[0], out[1]):
-        assert np.linalg.norm(a - b) <= 1e-4 * np.linalg.norm(a)
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(a)
 
 
 def test_zero_step_rollout_gradient_is_the_cotangent(nbb_mod):

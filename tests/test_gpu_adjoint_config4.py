@@ -17,10 +17,17 @@ in the differenced final states: with h = 1e-6 (1e-3 m) the smallest
 components (a mass gradient 100x below the median) come out 2e-3 off, while
 every component agrees to 5e-6 with the steps used here.
 
-Mixed rollout: its gradient is the FP64 vector-Jacobian product along the
-mixed trajectory (the FP32 interaction sums are not differentiated), held to
-the FP64 finite differences within MIXED_L2_BAR relative L2 over the 64
-coordinates.
+Mixed rollout: its gradient is the vector-Jacobian product of the mixed
+force itself (group-box acceptance, the mixed walk's interaction lists, FP32
+arithmetic) along the mixed trajectory.  Its position and velocity components
+are held to the FP64 finite differences within MIXED_L2_BAR relative L2.
+Its mass components are not: a mass derivative through a cell's monopole
+misses the cell's dipole-order term, so the mass gradients of two tree
+forces with different acceptance sets (the mixed form opens more cells)
+differ by a few percent.  Both tree gradients are instead held to the
+all-pairs FP64 adjoint (the exact gradient of the Newtonian rollout) under a
+linear loss: the mixed one within MIXED_DIRECT_BAR per kind and no farther
+than the plain tree gradient (with a 1.5x margin).
 """
 import numpy as np
 import pytest
@@ -33,6 +40,7 @@ EVERY = 32
 COORDS = 64
 FD_RTOL = 1e-5
 MIXED_L2_BAR = 1e-2
+MIXED_DIRECT_BAR = 5e-2
 
 
 def _perturbed(p, which, k, h):
@@ -118,4 +126,25 @@ def test_mixed_rollout_gradient_within_bar_of_finite_differences(nbb_mod, config
     p, target, coords, fd = config4
     ad = _pick(_gradient(nbb_mod, p, target, nbb_mod.PRECISION_MIXED), coords)
     assert np.all(np.isfinite(ad))
-    assert np.linalg.norm(ad - fd) <= MIXED_L2_BAR * np.linalg.norm(fd)
+    phase = np.array([w != "mass" for w, _ in coords])
+    assert np.linalg.norm(ad[phase] - fd[phase]) <= MIXED_L2_BAR * np.linalg.norm(fd[phase])
+
+
+def test_tree_gradients_against_all_pairs_adjoint(nbb_mod, config4):
+    p = config4[0]
+    rng = np.random.Generator(np.random.Philox(99))
+    wx = rng.standard_normal((3, N)) / N
+    wv = rng.standard_normal((3, N)) / N
+    cfg = nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0)
+    _, dm, dx, dv = nbb_mod.direct_rollout_adjoint(p, cfg, STEPS, wx, wv)
+    err = {}
+    for prec in (nbb_mod.PRECISION_FP64, nbb_mod.PRECISION_MIXED):
+        sim = nbb_mod.Simulation(p, nbb_mod.SimulationConfig(1e-3, 0.5, 0.01, 1.0, precision=prec))
+        sim.initialize()
+        sim.rollout(STEPS, EVERY)
+        gm, gx, gv = sim.backward(wx, wv)
+        sim.close()
+        err[prec] = [np.linalg.norm(a - b) / np.linalg.norm(b) for a, b in ((gm, dm), (gx, dx), (gv, dv))]
+    for kind, (e_plain, e_mixed) in enumerate(zip(err[nbb_mod.PRECISION_FP64], err[nbb_mod.PRECISION_MIXED])):
+        assert e_mixed <= MIXED_DIRECT_BAR, (kind, err)
+        assert e_mixed <= 1.5 * e_plain, (kind, err)
