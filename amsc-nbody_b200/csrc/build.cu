@@ -153,6 +153,8 @@ __global__ void __launch_bounds__(kBlock) kd_bbox_kernel(Workspace ws, double dt
         ws.y[i] = py;
         ws.z[i] = pz;
       }
+      // one 32-byte record per particle for the Morton-order gather
+      if (ws.pos4) ws.pos4[i] = make_double4(px, py, pz, 0.0);
       nf |= !(isfinite(px) && isfinite(py) && isfinite(pz));
     }
     if (!multi) {
@@ -1892,9 +1894,70 @@ __global__ void __launch_bounds__(kBlock) lo_leaf_kernel(Workspace ws, double th
   }
 }
 
+// One internal cell b of a level (children in the next level's range
+// [hi, end)): mass and centre of mass from the children's records in octant
+// order (octree_physics.cu:156-245), target-group marks, then the records.
+template <int kRecords>
+__device__ __forceinline__ void lo_level_cell(const Workspace &ws, int level, double theta, int b, int hi, int end,
+                                              int M) {
+  DevScalars *sc = ws.sc;
+  const int4 f = ws.lo_first[b];
+  const int c0 = f.y;
+  const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
+  if (c0 == c1) return;  // a leaf
+  const int4 q = ws.lo_last[b];
+  const int pf = f.x, skip = f.z, pe = q.x, pre = q.y;
+  if (pre < 0 || pre >= M || skip <= pre + 1 || skip > M || c0 < hi || c1 < c0 || c1 > end || c1 - c0 > 8 ||
+      pf < 0 || pe <= pf || pe > ws.n) {
+    record_error(sc, kStageLayout, 1);
+    return;
+  }
+  const int nk = c1 - c0;
+  // children in visit order: octant 7 -> 0, the children in descending key order
+  int *kids = ws.node_kids + (size_t)pre * 8;
+  // target groups (group_mark_kernel's rule): a whole system that is one
+  // group, else the starts of the children's runs
+  const int np = pe - pf;
+  const bool whole = lo_whole_group(ws, level, np, false);
+  if (whole && level == ws.sys_levels) ws.tflag[pf] = 1;
+  const bool virt = level < ws.sys_levels;
+  const bool merge = !virt && (np <= 1 || level - ws.sys_levels >= ws.group_depth);
+  const bool child_compact_level = level + 1 - ws.sys_levels >= ws.group_depth;
+  int run = 0;
+  double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    if (c0 + j < c1) {
+      const LevelNode ch = ws.lo_node[c0 + j];
+      const double cm = ch.a.w;
+      tm = __dadd_rn(tm, cm);
+      wx = __fma_rn(cm, ch.a.x, wx);
+      wy = __fma_rn(cm, ch.a.y, wy);
+      wz = __fma_rn(cm, ch.a.z, wz);
+      kids[nk - 1 - j] = ch.pre;
+      if (!whole) {
+        if (virt) run = 0;
+        const int cp = ch.np;
+        if (cp > ws.group_max || !(ch.leaf || cp <= 1 || child_compact_level)) {
+          run = 0;  // the child splits itself
+        } else {
+          if (!merge || run == 0 || run + cp > ws.group_max) {
+            if (ch.first >= 0 && ch.first < ws.n) ws.tflag[ch.first] = 1;
+            run = 0;
+          }
+          run += cp;
+        }
+      }
+    }
+  }
+  for (int j = nk; j < 8; ++j) kids[j] = -1;
+  const unsigned long long key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
+  if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key))
+    record_error(sc, kStageGeometry, 2);
+}
+
 // The internal cells of one level (deepest first; the leaves were finished
-// by lo_rank_kernel): mass and centre of mass from the children's records in
-// octant order (octree_physics.cu:156-245), then the cell's records.
+// by lo_leaf_kernel), one cell per thread.
 template <int kRecords>
 __global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int level, double theta) {
   __shared__ int s_lo, s_hi, s_end, s_m;
@@ -1922,60 +1985,42 @@ __global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int l
   }
   __syncthreads();
   const int lo = s_lo, hi = s_hi, end = s_end, M = s_m;
-  for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi; b += gridDim.x * blockDim.x) {
-    const int4 f = ws.lo_first[b];
-    const int c0 = f.y;
-    const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
-    if (c0 == c1) continue;  // a leaf
-    const int4 q = ws.lo_last[b];
-    const int pf = f.x, skip = f.z, pe = q.x, pre = q.y;
-    if (pre < 0 || pre >= M || skip <= pre + 1 || skip > M || c0 < hi || c1 < c0 || c1 > end || c1 - c0 > 8 ||
-        pf < 0 || pe <= pf || pe > ws.n) {
-      record_error(sc, kStageLayout, 1);
-      continue;
-    }
-    const int nk = c1 - c0;
-    // children in visit order: octant 7 -> 0, the children in descending key order
-    int *kids = ws.node_kids + (size_t)pre * 8;
-    // target groups (group_mark_kernel's rule): a whole system that is one
-    // group, else the starts of the children's runs
-    const int np = pe - pf;
-    const bool whole = lo_whole_group(ws, level, np, false);
-    if (whole && level == ws.sys_levels) ws.tflag[pf] = 1;
-    const bool virt = level < ws.sys_levels;
-    const bool merge = !virt && (np <= 1 || level - ws.sys_levels >= ws.group_depth);
-    const bool child_compact_level = level + 1 - ws.sys_levels >= ws.group_depth;
-    int run = 0;
-    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (c0 + j < c1) {
-        const LevelNode ch = ws.lo_node[c0 + j];
-        const double cm = ch.a.w;
-        tm = __dadd_rn(tm, cm);
-        wx = __fma_rn(cm, ch.a.x, wx);
-        wy = __fma_rn(cm, ch.a.y, wy);
-        wz = __fma_rn(cm, ch.a.z, wz);
-        kids[nk - 1 - j] = ch.pre;
-        if (!whole) {
-          if (virt) run = 0;
-          const int cp = ch.np;
-          if (cp > ws.group_max || !(ch.leaf || cp <= 1 || child_compact_level)) {
-            run = 0;  // the child splits itself
-          } else {
-            if (!merge || run == 0 || run + cp > ws.group_max) {
-              if (ch.first >= 0 && ch.first < ws.n) ws.tflag[ch.first] = 1;
-              run = 0;
-            }
-            run += cp;
-          }
+  for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi; b += gridDim.x * blockDim.x)
+    lo_level_cell<kRecords>(ws, level, theta, b, hi, end, M);
+}
+
+// The small top levels (top..0) in one block, level after level (a block
+// barrier between them): one launch instead of one per level.
+template <int kRecords>
+__global__ void __launch_bounds__(1024) lo_upper_levels_kernel(Workspace ws, int top, double theta) {
+  __shared__ int s_lo, s_hi, s_end, s_m;
+  DevScalars *sc = ws.sc;
+  for (int level = top; level >= 0; --level) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = 0, end = 0;
+      const int m = sc->n_nodes;
+      if (!sc->error && m > 0) {
+        long long bb = 0;
+        for (int l = 0; l < level; ++l) bb += sc->level_count[l];
+        const long long h = bb + sc->level_count[level];
+        const long long e = h + ((level + 1 < kMaxLevels) ? sc->level_count[level + 1] : 0);
+        if (e <= m) {
+          lo = (int)bb;
+          hi = (int)h;
+          end = (int)e;
+        } else {
+          record_error(sc, kStageLayout, 1);
         }
       }
+      s_lo = lo;
+      s_hi = hi;
+      s_end = end;
+      s_m = m;
     }
-    for (int j = nk; j < 8; ++j) kids[j] = -1;
-    const unsigned long long key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
-    if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key))
-      record_error(sc, kStageGeometry, 2);
+    __syncthreads();
+    const int lo = s_lo, hi = s_hi, end = s_end, M = s_m;
+    for (int b = lo + threadIdx.x; b < hi; b += blockDim.x) lo_level_cell<kRecords>(ws, level, theta, b, hi, end, M);
+    __syncthreads();
   }
 }
 
@@ -2156,6 +2201,20 @@ __global__ void __launch_bounds__(kBlock) gather_sorted_kernel(Workspace ws, con
   }
 }
 
+// The same gather from the kick-drift pass's {x, y, z} records: two reads
+// per particle instead of four (random reads are what this gather waits on).
+__global__ void __launch_bounds__(kBlock) gather_pos4_kernel(Workspace ws) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x) {
+    const uint32_t k = ws.idx[i];
+    if (k >= (uint32_t)ws.n) {
+      record_error(ws.sc, kStagePhysics, 3);
+      continue;
+    }
+    const double4 q = ws.pos4[k];
+    ws.pm4[i] = make_double4(q.x, q.y, q.z, ws.m[k]);
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) pack_keys_kernel(Workspace ws, const uint32_t *keys) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ws.n; i += gridDim.x * blockDim.x)
     ws.pairs_a[i] = ((unsigned long long)keys[i] << ws.pack_shift) | (unsigned)i;
@@ -2217,8 +2276,11 @@ cudaError_t launch_morton_sort_groups(Workspace &ws, cudaStream_t s, int part) {
     groups_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, sorted, 0);
     // the first reader of the masses: the Morton-order gather, one particle
     // per thread so that every thread's four loads are in flight at once
-    gather_sorted_kernel<<<(ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1, kBlock, 0, s>>>(
-        ws, ws.idx);
+    const int blocks = (ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1;
+    if (ws.pos4)
+      gather_pos4_kernel<<<blocks, kBlock, 0, s>>>(ws);
+    else
+      gather_sorted_kernel<<<blocks, kBlock, 0, s>>>(ws, ws.idx);
     count_launches(2);
   }
   return cudaGetLastError();
@@ -2272,8 +2334,12 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     lo_leaf_kernel<kRecordsFp64><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
   else
     lo_leaf_kernel<kRecordsFp64 | kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
-  // the deepest level holds only leaves
-  for (int level = ws.max_level - 1; level >= 0; --level) {
+  // the deepest level holds only leaves; levels kUpperLevels..0 (at most 73
+  // cells) share one block (a single block for levels up to 4 measured
+  // slower than their own launches: 54 against 41 us)
+  constexpr int kUpperLevels = 2;
+  const int split = kUpperLevels < ws.max_level - 1 ? kUpperLevels : ws.max_level - 1;
+  for (int level = ws.max_level - 1; level > split; --level) {
     if (ws.records == kRecordsMixed)
       lo_level_kernel<kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
     else if (ws.records == kRecordsFp64)
@@ -2281,13 +2347,19 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     else
       lo_level_kernel<kRecordsFp64 | kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
   }
+  if (ws.records == kRecordsMixed)
+    lo_upper_levels_kernel<kRecordsMixed><<<1, 1024, 0, s>>>(ws, split, theta);
+  else if (ws.records == kRecordsFp64)
+    lo_upper_levels_kernel<kRecordsFp64><<<1, 1024, 0, s>>>(ws, split, theta);
+  else
+    lo_upper_levels_kernel<kRecordsFp64 | kRecordsMixed><<<1, 1024, 0, s>>>(ws, split, theta);
   if (ws.top && (ws.records & kRecordsMixed) && ws.n_systems == 1) {
     lo_top_kernel<<<1, 128, 0, s>>>(ws);
     count_launches(1);
   }
   // target-group marks were set by the leaf and level passes
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(5 + ws.max_level);
+  count_launches(5 + ws.max_level - split);
   return cudaGetLastError();
 }
 

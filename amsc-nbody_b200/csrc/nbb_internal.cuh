@@ -229,6 +229,7 @@ struct Workspace {
   int4 *lo_first = nullptr;     // cap: first particle, first child, subtree end (preorder), first group
   int4 *lo_last = nullptr;      // cap: particle end, preorder index, key (low, high 32 bits)
   int2 *lo_gleaf = nullptr;     // n: per group, its leaf's level-order index and S(g)
+  double4 *pos4 = nullptr;      // n: {x, y, z, -} in original order, written by the kick-drift pass
   LevelNode *lo_node = nullptr;  // cap: mass, centre of mass, preorder index, particles
   int *lo_tiles = nullptr;      // scan_tiles_n * kLevelOrderChannels: per-tile counts, then their prefixes
   int records = kRecordsFp64 | kRecordsMixed;  // host: the records the level-order build writes

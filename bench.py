@@ -327,16 +327,19 @@ def run_nbb(args, rank, world, local):
 
 
 # Algorithmic bytes of the step's rebuild (the level-order build of a mixed
-# step): per particle, per unique-key group and per octree node, each term the
-# sum of the arrays that stage must read once and write once.
-BUILD_BYTES_PER_PARTICLE = 120 + 32 + 64 + 80 + 32  # KD+bbox, encode, 4 sort passes, groups+gather, leaf mass
-BUILD_BYTES_PER_GROUP = 24 + 20                     # level spans + counts, cell ranks (group payloads)
-BUILD_BYTES_PER_OCTREE_NODE = 32 + 208 + 112        # cell entries; level pass (entries, child records,
-                                                    # LevelNode, MixedNode, child list); target-group marks
+# step): per particle, per unique-key group (= occupied leaf), per octree node
+# and per internal node, each term the sum of the arrays that kernel must read
+# once and write once.
+BUILD_BYTES_PER_PARTICLE = (152 + 32 + 4 * 16     # kick-drift + box (+ position records), encode, 4 sort passes
+                            + 20 + 76 + 32 + 1)   # groups, Morton gather, leaf mass, target-group scan
+BUILD_BYTES_PER_GROUP = 16 + 24 + 20 + 124        # group arrays, level spans, cell ranks, leaf records
+BUILD_BYTES_PER_OCTREE_NODE = 32 + 48             # cell entries, read once as a child
+BUILD_BYTES_PER_INTERNAL_NODE = 160               # level pass: entries, LevelNode, MixedNode, child list
 
 
 def build_algorithmic_bytes(n, groups, nodes):
-    return BUILD_BYTES_PER_PARTICLE * n + BUILD_BYTES_PER_GROUP * groups + BUILD_BYTES_PER_OCTREE_NODE * nodes
+    return (BUILD_BYTES_PER_PARTICLE * n + BUILD_BYTES_PER_GROUP * groups + BUILD_BYTES_PER_OCTREE_NODE * nodes
+            + BUILD_BYTES_PER_INTERNAL_NODE * max(nodes - groups, 0))
 
 
 def load_peaks():
