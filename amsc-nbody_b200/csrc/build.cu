@@ -76,6 +76,7 @@ __global__ void reset_scalars_kernel(DevScalars *sc) {
     sc->interactions = 0;
     sc->mac_tests = 0;
     for (int l = 0; l < kMaxLevels; ++l) sc->level_count[l] = 0;
+    for (int l = 0; l < kMaxLevels + 2; ++l) sc->level_base[l] = 0;
   }
 }
 
@@ -1047,7 +1048,7 @@ __global__ void __launch_bounds__(kBlock) node_init_kernel(Workspace ws) {
     }
     ws.mass[node] = tm;
     if (tm > 0.0) {
-      const double inv = __ddiv_rn(1.0, tm);
+      const double inv = __drcp_rn(tm);
       ws.comx[node] = __dmul_rn(wx, inv);
       ws.comy[node] = __dmul_rn(wy, inv);
       ws.comz[node] = __dmul_rn(wz, inv);
@@ -1168,7 +1169,7 @@ __global__ void __launch_bounds__(kBlock) propagate_level_kernel(Workspace ws, i
     }
     ws.mass[node] = tm;
     if (tm > 0.0) {
-      const double inv = __ddiv_rn(1.0, tm);
+      const double inv = __drcp_rn(tm);
       ws.comx[node] = __dmul_rn(wx, inv);
       ws.comy[node] = __dmul_rn(wy, inv);
       ws.comz[node] = __dmul_rn(wz, inv);
@@ -1573,8 +1574,10 @@ __global__ void __launch_bounds__(32 * kLevelOrderChannels) lo_tile_scan_kernel(
     long long m = 0;
     for (int l = 0; l < kMaxLevels; ++l) {
       sc->level_count[l] = (int)s_total[l];
+      sc->level_base[l] = (int)m;
       m += s_total[l];
     }
+    sc->level_base[kMaxLevels] = sc->level_base[kMaxLevels + 1] = (int)m;
     if (G == 0 || m != s_total[kEnded] || m > ws.cap_nodes) {
       if (G > 0) record_error(sc, m > ws.cap_nodes ? kStagePlan : kStageLayout, m > ws.cap_nodes ? kCodeOverflow : 1);
       sc->n_nodes = 0;
@@ -1596,7 +1599,7 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
                                         double wz, unsigned long long key) {
   double comx = 0.0, comy = 0.0, comz = 0.0;
   if (tm > 0.0) {
-    const double inv = __ddiv_rn(1.0, tm);
+    const double inv = __drcp_rn(tm);
     comx = __dmul_rn(wx, inv);
     comy = __dmul_rn(wy, inv);
     comz = __dmul_rn(wz, inv);
@@ -1665,7 +1668,8 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
 
 // Cell numbers: per tile, the cells started by the groups before it (the
 // tile prefixes) plus the ranks inside the tile.  Writes each cell's first
-// particle, first child, subtree end and first group (by its first group) and
+// particle, first child, subtree end and parent, and zeroes its arrival
+// counter (by its first group), and
 // its particle end, preorder index and key (by its last group; every group of
 // a cell carries the cell's prefix), and per group its leaf's level-order
 // index and S(g) (the leaf sits at level lambda, preorder index S(g) - 1).
@@ -1682,16 +1686,13 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
   DevScalars *sc = ws.sc;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile = blockIdx.x;
+  // the level bases, one load per thread (a serial loop of dependent
+  // additions over the level counts would cost a memory round trip each)
+  if (tid < kMaxLevels + 2) s_base[tid] = sc->level_base[tid];
   if (tid == 0) {
     const int g = sc->n_groups, m = sc->n_nodes;
     s_g = (g > 0 && g <= ws.n && m > 0) ? g : 0;
     s_m = m;
-    int run = 0;
-    for (int l = 0; l < kMaxLevels; ++l) {
-      s_base[l] = run;
-      run += sc->level_count[l];
-    }
-    s_base[kMaxLevels] = s_base[kMaxLevels + 1] = run;
   }
   if (tid < kLevelOrderChannels) s_prefix[tid] = ws.lo_tiles[(size_t)tile * kLevelOrderChannels + tid];
   __syncthreads();
@@ -1739,13 +1740,14 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
     for (int l = 0; l < kMaxLevels; ++l) cnt[l] += (int)((sm >> l) & 1u);
     e += __popc(lm);
   }
-  // the warp's level range: ranks are formed only where its groups have cells
+  // the warp's level range: ranks are formed only where its groups have
+  // cells, and at the level above (the parent of a group's shallowest cell)
   int wlo = kMaxLevels, whi = -1;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
     if (span[k] < 0) continue;
     const int d = (span[k] & 255) - 1, l = (span[k] >> 8) & 255, dn = ((span[k] >> 16) & 255) - 1;
-    wlo = min(wlo, min(d, dn) + 1);
+    wlo = min(wlo, max(0, min(d, dn)));
     whi = max(whi, l + 1);
   }
   wlo = __reduce_min_sync(0xffffffffu, wlo);
@@ -1810,14 +1812,22 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
     excl[kMaxLevels] = 0;
     if (lam == 0) continue;
     int bleaf = -1;
+    const int delta = (sp & 255) - 1;
 #pragma unroll
     for (int l = 0; l < kMaxLevels; ++l) {
       if (l < wlo || l > whi) continue;
       const int started = (int)((sm >> l) & 1u);
       if (started) {
         const int b = s_base[l] + excl[l];
-        if (b < s_base[l + 1]) ws.lo_first[b] = make_int4(pf, s_base[l + 1] + excl[l + 1], s_from, g);
-        else record_error(sc, kStageLayout, 1);
+        // the parent: started by this group too, or (one level below the
+        // common levels) the last cell started before it at level delta
+        const int parent = (l == 0) ? -1 : s_base[l - 1] + excl[l - 1] - (l - 1 == delta ? 1 : 0);
+        if (b < s_base[l + 1]) {
+          ws.lo_first[b] = make_int4(pf, s_base[l + 1] + excl[l + 1], s_from, parent);
+          ws.lo_arrive[b] = 0;
+        } else {
+          record_error(sc, kStageLayout, 1);
+        }
         if (l == lam) bleaf = b;
       }
       if (((lm >> l) & 1u) && l < lam) {
@@ -1829,7 +1839,7 @@ __global__ void __launch_bounds__(kScanThreads) lo_rank_kernel(Workspace ws, dou
           record_error(sc, kStageLayout, 1);
       }
     }
-    // the leaf (level lambda, preorder index S(g) - 1), finished by lo_leaf_kernel
+    // the leaf (level lambda, preorder index S(g) - 1), finished by lo_upsweep_kernel
     if (bleaf < 0 || s_from < 1 || s_from > M) {
       record_error(sc, kStageLayout, 1);
       continue;
@@ -1849,68 +1859,76 @@ __device__ __forceinline__ bool lo_whole_group(const Workspace &ws, int level, i
   return !virt && np <= ws.group_max && compact;
 }
 
-// Occupied leaves, one group per thread: mass and centre of mass of the
-// group's particles in sorted order (octree_physics.cu:95-154), the leaf's
-// records at preorder index S(g) - 1 (no child list: neither walk reads one
-// for an occupied leaf), and its target-group marks.
+// A child's LevelNode, written earlier in the same kernel by another thread
+// of the upward pass: read from L2 (ld.global.cg), never from a stale L1 line.
+__device__ __forceinline__ LevelNode ld_level_node_cg(const LevelNode *p) {
+  const double2 *d = reinterpret_cast<const double2 *>(p);
+  const double2 lo = __ldcg(d), hi = __ldcg(d + 1);
+  const int4 t = __ldcg(reinterpret_cast<const int4 *>(p) + 2);
+  LevelNode r;
+  r.a = make_double4(lo.x, lo.y, hi.x, hi.y);
+  r.pre = t.x;
+  r.np = t.y;
+  r.first = t.z;
+  r.leaf = t.w;
+  return r;
+}
+
+// The occupied leaf of group g: mass and centre of mass of the group's
+// particles in sorted order (octree_physics.cu:95-154), the leaf's records at
+// preorder index S(g) - 1 (no child list: neither walk reads one for an
+// occupied leaf), and its target-group marks.  Returns the leaf's level-order
+// index and level, or false on inconsistent input.
 template <int kRecords>
-__global__ void __launch_bounds__(kBlock) lo_leaf_kernel(Workspace ws, double theta) {
-  __shared__ int s_g, s_m;
+__device__ __forceinline__ bool lo_leaf_cell(const Workspace &ws, double theta, int g, int M, int &bleaf, int &lam) {
   DevScalars *sc = ws.sc;
-  if (threadIdx.x == 0) {
-    const int g = sc->n_groups, m = sc->n_nodes;
-    s_g = (!sc->error && g > 0 && g <= ws.n && m > 0) ? g : 0;
-    s_m = m;
+  const int2 lf = ws.lo_gleaf[g];
+  const int pf = ws.gfirst[g], pe = ws.glast[g] + 1;
+  const unsigned long long key = ws.ukey[g];
+  lam = (ws.gspan[g] >> 8) & 255;
+  bleaf = lf.x;
+  const int skip = lf.y, pre = skip - 1;
+  if (bleaf < 0 || bleaf >= M || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n || lam < 1 ||
+      lam > ws.max_level) {
+    record_error(sc, kStageLayout, 1);
+    return false;
   }
-  __syncthreads();
-  const int G = s_g, M = s_m;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
-    const int2 lf = ws.lo_gleaf[g];
-    const int pf = ws.gfirst[g], pe = ws.glast[g] + 1;
-    const unsigned long long key = ws.ukey[g];
-    const int lam = (ws.gspan[g] >> 8) & 255;
-    const int bleaf = lf.x, skip = lf.y, pre = skip - 1;
-    if (bleaf < 0 || bleaf >= M || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n ||
-        lam < 1 || lam > ws.max_level) {
-      record_error(sc, kStageLayout, 1);
-      continue;
-    }
-    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-    for (int i = pf; i < pe; ++i) {
-      const double4 q = ws.pm4[i];
-      tm = __dadd_rn(tm, q.w);
-      wx = __fma_rn(q.w, q.x, wx);
-      wy = __fma_rn(q.w, q.y, wy);
-      wz = __fma_rn(q.w, q.z, wz);
-    }
-    if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, skip, pf, pe, true, 0, tm, wx, wy, wz, key))
-      record_error(sc, kStageGeometry, 2);
-    const int np = pe - pf;
-    if (lo_whole_group(ws, lam, np, true)) {
-      if (lam == ws.sys_levels) ws.tflag[pf] = 1;
-    } else {
-      for (int k = 0; k < np; k += ws.group_max) ws.tflag[pf + k] = 1;
-    }
+  double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  for (int i = pf; i < pe; ++i) {
+    const double4 q = ws.pm4[i];
+    tm = __dadd_rn(tm, q.w);
+    wx = __fma_rn(q.w, q.x, wx);
+    wy = __fma_rn(q.w, q.y, wy);
+    wz = __fma_rn(q.w, q.z, wz);
   }
+  if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, skip, pf, pe, true, 0, tm, wx, wy, wz, key)) {
+    record_error(sc, kStageGeometry, 2);
+    return false;
+  }
+  const int np = pe - pf;
+  if (lo_whole_group(ws, lam, np, true)) {
+    if (lam == ws.sys_levels) ws.tflag[pf] = 1;
+  } else {
+    for (int k = 0; k < np; k += ws.group_max) ws.tflag[pf + k] = 1;
+  }
+  return true;
 }
 
 // One internal cell b of a level (children in the next level's range
 // [hi, end)): mass and centre of mass from the children's records in octant
 // order (octree_physics.cu:156-245), target-group marks, then the records.
+// Returns false on inconsistent input.
 template <int kRecords>
-__device__ __forceinline__ void lo_level_cell(const Workspace &ws, int level, double theta, int b, int hi, int end,
-                                              int M) {
+__device__ __forceinline__ bool lo_level_cell(const Workspace &ws, int level, double theta, int b, int hi, int end,
+                                              int M, const int4 &f, const int4 &q, int next_first_child) {
   DevScalars *sc = ws.sc;
-  const int4 f = ws.lo_first[b];
   const int c0 = f.y;
-  const int c1 = (b + 1 < hi) ? ws.lo_first[b + 1].y : end;
-  if (c0 == c1) return;  // a leaf
-  const int4 q = ws.lo_last[b];
+  const int c1 = (b + 1 < hi) ? next_first_child : end;
   const int pf = f.x, skip = f.z, pe = q.x, pre = q.y;
-  if (pre < 0 || pre >= M || skip <= pre + 1 || skip > M || c0 < hi || c1 < c0 || c1 > end || c1 - c0 > 8 ||
+  if (pre < 0 || pre >= M || skip <= pre + 1 || skip > M || c0 < hi || c1 <= c0 || c1 > end || c1 - c0 > 8 ||
       pf < 0 || pe <= pf || pe > ws.n) {
     record_error(sc, kStageLayout, 1);
-    return;
+    return false;
   }
   const int nk = c1 - c0;
   // children in visit order: octant 7 -> 0, the children in descending key order
@@ -1928,7 +1946,7 @@ __device__ __forceinline__ void lo_level_cell(const Workspace &ws, int level, do
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     if (c0 + j < c1) {
-      const LevelNode ch = ws.lo_node[c0 + j];
+      const LevelNode ch = ld_level_node_cg(ws.lo_node + c0 + j);
       const double cm = ch.a.w;
       tm = __dadd_rn(tm, cm);
       wx = __fma_rn(cm, ch.a.x, wx);
@@ -1952,75 +1970,97 @@ __device__ __forceinline__ void lo_level_cell(const Workspace &ws, int level, do
   }
   for (int j = nk; j < 8; ++j) kids[j] = -1;
   const unsigned long long key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
-  if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key))
+  if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key)) {
     record_error(sc, kStageGeometry, 2);
+    return false;
+  }
+  return true;
 }
 
-// The internal cells of one level (deepest first; the leaves were finished
-// by lo_leaf_kernel), one cell per thread.
+// Atomic addition with acquire-release semantics at GPU scope: the adding
+// thread's earlier writes are visible to any thread that later observes the
+// sum, and this thread's later reads see what the earlier adders wrote.
+__device__ __forceinline__ unsigned atomic_add_acq_rel(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// A cell's arrival at its parent p.  The children of p are the consecutive
+// cells [c0, c1) of the next level; child c adds 1, plus c if it is the first
+// child (the cell before it has another parent) and 2^31 - (c + 1) if it is
+// the last.  The counter (zeroed by lo_rank) reaches 2^31 exactly when every
+// child has added, (c1 - c0) + c0 + 2^31 - c1, and stays below it before, so
+// the child count is not needed to detect the last arrival.  Returns whether
+// this cell arrived last.
+__device__ __forceinline__ bool lo_arrive_last(const Workspace &ws, int c, int p, int left_parent, int right_parent,
+                                               bool &bad) {
+  constexpr unsigned kDone = 0x80000000u;
+  const unsigned add = 1u + (left_parent != p ? (unsigned)c : 0u) + (right_parent != p ? kDone - (unsigned)(c + 1) : 0u);
+  const unsigned sum = atomic_add_acq_rel(reinterpret_cast<unsigned *>(ws.lo_arrive) + p, add) + add;
+  bad = sum > kDone;
+  return sum == kDone;
+}
+
+// The whole upward pass in one launch, with arrival counters instead of one
+// launch per level: a thread finishes the leaf of group g, then climbs.  At
+// each parent it counts itself in (lo_arrive_last: an acquire-release atomic
+// publishes the child's records); the child that arrives last finishes the
+// parent from its children's records and climbs on, the others stop.  Every
+// cell is finished exactly once, after all of its children, with the same
+// arithmetic in the same child order as a level-by-level pass.  No thread
+// ever waits: a climb ends at the root, at a parent that other children
+// still owe, or at the first inconsistency.
 template <int kRecords>
-__global__ void __launch_bounds__(kBlock, 4) lo_level_kernel(Workspace ws, int level, double theta) {
-  __shared__ int s_lo, s_hi, s_end, s_m;
+__global__ void __launch_bounds__(kBlock, 4) lo_upsweep_kernel(Workspace ws, double theta) {
+  __shared__ int s_g, s_m;
+  __shared__ int s_base[kMaxLevels + 2];
   DevScalars *sc = ws.sc;
+  if (threadIdx.x < kMaxLevels + 2) s_base[threadIdx.x] = sc->level_base[threadIdx.x];
   if (threadIdx.x == 0) {
-    int lo = 0, hi = 0, end = 0;
-    const int m = sc->n_nodes;
-    if (!sc->error && m > 0) {
-      long long b = 0;
-      for (int l = 0; l < level; ++l) b += sc->level_count[l];
-      const long long h = b + sc->level_count[level];
-      const long long e = h + ((level + 1 < kMaxLevels) ? sc->level_count[level + 1] : 0);
-      if (e <= m) {
-        lo = (int)b;
-        hi = (int)h;
-        end = (int)e;
-      } else {
-        record_error(sc, kStageLayout, 1);
-      }
-    }
-    s_lo = lo;
-    s_hi = hi;
-    s_end = end;
+    const int g = sc->n_groups, m = sc->n_nodes;
+    s_g = (!sc->error && g > 0 && g <= ws.n && m > 0) ? g : 0;
     s_m = m;
   }
   __syncthreads();
-  const int lo = s_lo, hi = s_hi, end = s_end, M = s_m;
-  for (int b = lo + blockIdx.x * blockDim.x + threadIdx.x; b < hi; b += gridDim.x * blockDim.x)
-    lo_level_cell<kRecords>(ws, level, theta, b, hi, end, M);
-}
-
-// The small top levels (top..0) in one block, level after level (a block
-// barrier between them): one launch instead of one per level.
-template <int kRecords>
-__global__ void __launch_bounds__(1024) lo_upper_levels_kernel(Workspace ws, int top, double theta) {
-  __shared__ int s_lo, s_hi, s_end, s_m;
-  DevScalars *sc = ws.sc;
-  for (int level = top; level >= 0; --level) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = 0, end = 0;
-      const int m = sc->n_nodes;
-      if (!sc->error && m > 0) {
-        long long bb = 0;
-        for (int l = 0; l < level; ++l) bb += sc->level_count[l];
-        const long long h = bb + sc->level_count[level];
-        const long long e = h + ((level + 1 < kMaxLevels) ? sc->level_count[level + 1] : 0);
-        if (e <= m) {
-          lo = (int)bb;
-          hi = (int)h;
-          end = (int)e;
-        } else {
-          record_error(sc, kStageLayout, 1);
-        }
+  const int G = s_g, M = s_m;
+  if (G > 0 && s_base[kMaxLevels] != M) {
+    if (threadIdx.x == 0) record_error(sc, kStageLayout, 1);
+    return;
+  }
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    int cell, level;
+    if (!lo_leaf_cell<kRecords>(ws, theta, g, M, cell, level)) continue;
+    // the cell's parent and its neighbours' (which children are first and last)
+    int p = ws.lo_first[cell].w;
+    int pl = cell > s_base[level] ? ws.lo_first[cell - 1].w : -1;
+    int pr = cell + 1 < s_base[level + 1] ? ws.lo_first[cell + 1].w : -1;
+    while (level > 0) {
+      const int lv = level - 1;
+      const int lo = s_base[lv], hi = s_base[lv + 1], end = s_base[lv + 2];
+      if (p < lo || p >= hi) {
+        record_error(sc, kStageLayout, 1);
+        break;
       }
-      s_lo = lo;
-      s_hi = hi;
-      s_end = end;
-      s_m = m;
+      bool bad;
+      const bool last = lo_arrive_last(ws, cell, p, pl, pr, bad);
+      if (!last) {
+        if (bad) record_error(sc, kStageLayout, 1);
+        break;
+      }
+      // the parent's entries, its successor's first child and the parents of
+      // its neighbours, in one round trip
+      const int4 f = ws.lo_first[p];
+      const int4 q = ws.lo_last[p];
+      const int4 fr = (p + 1 < hi) ? ws.lo_first[p + 1] : make_int4(0, end, 0, -1);
+      const int npl = p > lo ? ws.lo_first[p - 1].w : -1;
+      if (!lo_level_cell<kRecords>(ws, lv, theta, p, hi, end, M, f, q, fr.y)) break;
+      cell = p;
+      level = lv;
+      p = f.w;
+      pl = npl;
+      pr = fr.w;
     }
-    __syncthreads();
-    const int lo = s_lo, hi = s_hi, end = s_end, M = s_m;
-    for (int b = lo + threadIdx.x; b < hi; b += blockDim.x) lo_level_cell<kRecords>(ws, level, theta, b, hi, end, M);
-    __syncthreads();
   }
 }
 
@@ -2030,14 +2070,10 @@ __global__ void __launch_bounds__(kBlock) lo_group_mark_kernel(Workspace ws) {
   __shared__ int s_base[kMaxLevels + 2];
   __shared__ int s_m;
   DevScalars *sc = ws.sc;
+  if (threadIdx.x < kMaxLevels + 2) s_base[threadIdx.x] = sc->level_base[threadIdx.x];
   if (threadIdx.x == 0) {
-    int run = 0;
-    for (int l = 0; l < kMaxLevels; ++l) {
-      s_base[l] = run;
-      run += sc->level_count[l];
-    }
-    s_base[kMaxLevels] = s_base[kMaxLevels + 1] = run;
-    s_m = (sc->error || sc->n_nodes != run) ? 0 : run;
+    const int m = sc->n_nodes;
+    s_m = (sc->error || m != sc->level_base[kMaxLevels]) ? 0 : m;
   }
   __syncthreads();
   const int M = s_m, gmax = ws.group_max, n = ws.n;
@@ -2093,14 +2129,10 @@ __global__ void __launch_bounds__(128) lo_top_kernel(Workspace ws) {
   __shared__ int s_base[kTopDepth + 3];
   __shared__ int s_ok;
   DevScalars *sc = ws.sc;
+  if (threadIdx.x < kTopDepth + 3) s_base[threadIdx.x] = sc->level_base[threadIdx.x];
   if (threadIdx.x == 0) {
-    int run = 0;
-    for (int l = 0; l <= kTopDepth + 1; ++l) {
-      s_base[l] = run;
-      run += sc->level_count[l];
-    }
-    s_base[kTopDepth + 2] = run;
-    s_ok = !sc->error && sc->n_nodes > 0 && run <= sc->n_nodes;
+    const int m = sc->n_nodes;
+    s_ok = !sc->error && m > 0 && sc->level_base[kTopDepth + 2] <= m;
   }
   __syncthreads();
   if (!s_ok) return;
@@ -2327,39 +2359,23 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
     lo_rank_kernel<kRecordsFp64><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
   else
     lo_rank_kernel<kRecordsFp64 | kRecordsMixed><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
+  // leaves and every internal cell in one launch (arrival counters), one
+  // thread per group (a resident grid taking groups grid-stride measured
+  // slower: 267 against 174 us at 2^20 particles)
   const int leaf_grid = (ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1;
   if (ws.records == kRecordsMixed)
-    lo_leaf_kernel<kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+    lo_upsweep_kernel<kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
   else if (ws.records == kRecordsFp64)
-    lo_leaf_kernel<kRecordsFp64><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+    lo_upsweep_kernel<kRecordsFp64><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
   else
-    lo_leaf_kernel<kRecordsFp64 | kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
-  // the deepest level holds only leaves; levels kUpperLevels..0 (at most 73
-  // cells) share one block (a single block for levels up to 4 measured
-  // slower than their own launches: 54 against 41 us)
-  constexpr int kUpperLevels = 2;
-  const int split = kUpperLevels < ws.max_level - 1 ? kUpperLevels : ws.max_level - 1;
-  for (int level = ws.max_level - 1; level > split; --level) {
-    if (ws.records == kRecordsMixed)
-      lo_level_kernel<kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
-    else if (ws.records == kRecordsFp64)
-      lo_level_kernel<kRecordsFp64><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
-    else
-      lo_level_kernel<kRecordsFp64 | kRecordsMixed><<<level_grid(ws, level), kBlock, 0, s>>>(ws, level, theta);
-  }
-  if (ws.records == kRecordsMixed)
-    lo_upper_levels_kernel<kRecordsMixed><<<1, 1024, 0, s>>>(ws, split, theta);
-  else if (ws.records == kRecordsFp64)
-    lo_upper_levels_kernel<kRecordsFp64><<<1, 1024, 0, s>>>(ws, split, theta);
-  else
-    lo_upper_levels_kernel<kRecordsFp64 | kRecordsMixed><<<1, 1024, 0, s>>>(ws, split, theta);
+    lo_upsweep_kernel<kRecordsFp64 | kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
   if (ws.top && (ws.records & kRecordsMixed) && ws.n_systems == 1) {
     lo_top_kernel<<<1, 128, 0, s>>>(ws);
     count_launches(1);
   }
-  // target-group marks were set by the leaf and level passes
+  // target-group marks were set by the upward pass
   group_scan_kernel<<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws);
-  count_launches(5 + ws.max_level - split);
+  count_launches(5);
   return cudaGetLastError();
 }
 

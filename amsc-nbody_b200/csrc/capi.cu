@@ -225,7 +225,7 @@ cudaError_t alloc_workspace(Workspace &ws, Allocation &al, int n, bool with_stat
   if (level_order) {
     ws.level_order = 1;
     GET(ws.gspan, N);
-    GET(ws.lo_first, C); GET(ws.lo_last, C); GET(ws.lo_node, C); GET(ws.lo_gleaf, N);
+    GET(ws.lo_first, C); GET(ws.lo_arrive, C); GET(ws.lo_last, C); GET(ws.lo_node, C); GET(ws.lo_gleaf, N);
     GET(ws.pos4, N);
     GET(ws.lo_tiles, (size_t)ws.scan_tiles_n * kLevelOrderChannels);
     GET(ws.top, (size_t)kTopMax);

@@ -50,6 +50,7 @@ struct DevScalars {
   unsigned long long interactions;
   unsigned long long mac_tests;
   int level_count[16];           // octree nodes per level (kMaxLevels)
+  int level_base[18];            // level-order index of each level's first node (kMaxLevels + 2)
 };
 
 // Sort tiling (onesweep LSD radix sort of packed (key << 32 | index)).
@@ -226,7 +227,8 @@ struct Workspace {
   // level-order build (simulation steps): the octree numbered level by level
   int level_order = 0;          // host: 1 when steps build the level-order octree
   int *gspan = nullptr;         // n: per group (delta + 1) | lambda << 8 | (delta_next + 1) << 16
-  int4 *lo_first = nullptr;     // cap: first particle, first child, subtree end (preorder), first group
+  int4 *lo_first = nullptr;     // cap: first particle, first child, subtree end (preorder), parent
+  int *lo_arrive = nullptr;     // cap: children finished (arrival counters of the upward pass)
   int4 *lo_last = nullptr;      // cap: particle end, preorder index, key (low, high 32 bits)
   int2 *lo_gleaf = nullptr;     // n: per group, its leaf's level-order index and S(g)
   double4 *pos4 = nullptr;      // n: {x, y, z, -} in original order, written by the kick-drift pass

@@ -13,7 +13,6 @@
 #include "nbb_internal.cuh"
 
 #include <cmath>
-#include <mutex>
 #include <string>
 
 namespace {
@@ -38,12 +37,10 @@ constexpr size_t kOffPairsB = round_up(kOffPairsA + sizeof(unsigned long long) *
 constexpr size_t kScratchBytes = round_up(kOffPairsB + sizeof(unsigned long long) * kMaxN);
 
 // The scratch array.  In host code this name is only a host-side stand-in:
-// its device address comes from cudaGetSymbolAddress, per device.
+// its device address comes from cudaGetSymbolAddress in the current context,
+// asked on every call (no address is cached: a reset device or another
+// context on the same device has its own instance of the module).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
 
 thread_local std::string t_msg;
 
@@ -68,21 +65,21 @@ int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z, s
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(NBB_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return fail(NBB_ERR_CUDA, "device ordinal out of range");
-  unsigned char *base = nullptr;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   {
-    // set-up, once per device, with that device current: the device address
-    // of the scratch array
-    std::lock_guard<std::mutex> guard(g_lock);
-    if (!g_scratch_ptr[dev]) {
-      void *p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess)
-        return fail(NBB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
-    }
-    base = g_scratch_ptr[dev];
+    // the call ends with a device-to-host read and a stream synchronisation,
+    // neither of which a stream capture allows
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess)
+      return fail(NBB_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(NBB_ERR_INVALID_ARGUMENT, "nbb_morton_sort_noalloc cannot be captured in a CUDA graph");
   }
+  void *p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return fail(NBB_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  unsigned char *base = static_cast<unsigned char *>(p);
   Workspace ws{};
   ws.n = (int)n;
   cudaDeviceGetAttribute(&ws.num_sms, cudaDevAttrMultiProcessorCount, dev);
@@ -97,7 +94,6 @@ int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z, s
   ws.sort_status = reinterpret_cast<uint32_t *>(base + kOffStatus);
   ws.pairs_a = reinterpret_cast<unsigned long long *>(base + kOffPairsA);
   ws.pairs_b = reinterpret_cast<unsigned long long *>(base + kOffPairsB);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the sticky error word must start at zero for this call
   e = cudaMemsetAsync(&ws.sc->error, 0, sizeof(int), s);
   if (e == cudaSuccess) e = nbb::launch_morton_sort_only(ws, keys, idx, s);

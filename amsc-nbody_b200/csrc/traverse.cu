@@ -548,9 +548,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
   int ccount = 0;
   if (p.cache_depth > 0 && ws.top && ws.n_systems == 1) {
     if (threadIdx.x == 0) {
-      int cnt = 0;
-      for (int l = 0; l <= p.cache_depth && l <= kTopDepth; ++l) cnt += sc->level_count[l];
-      s_ccount = min(cnt, kTopMax);
+      s_ccount = min(sc->level_base[min(p.cache_depth, kTopDepth) + 1], kTopMax);
     }
     __syncthreads();
     ccount = s_ccount;
@@ -986,7 +984,7 @@ __global__ void __launch_bounds__(kDirectThreads)
         const double4 s = tile[q];
         const double dx = __dsub_rn(s.x, tx), dy = __dsub_rn(s.y, ty), dz = __dsub_rn(s.z, tz);
         const double d2 = __dadd_rn(sqdist(dx, dy, dz), soft2);
-        const double inv = __ddiv_rn(1.0, __dsqrt_rn(d2));
+        const double inv = __drcp_rn(__dsqrt_rn(d2));
         const double f = __dmul_rn(__dmul_rn(g, s.w), __dmul_rn(__dmul_rn(inv, inv), inv));
         rx = __fma_rn(f, dx, rx);
         ry = __fma_rn(f, dy, ry);

@@ -8,10 +8,13 @@
 namespace nbb {
 
 // barnes_hut.cu:56-80, the factor G m (d^2 + eps^2)^-3/2 with the
-// reference's operation order.  Returns false on a singular interaction.
+// reference's operation order.  The reference's 1.0 / sqrt(r2) is a
+// correctly rounded division of 1, which is the correctly rounded reciprocal
+// (__drcp_rn, a shorter sequence than the general division): the same bits
+// for every input.  Returns false on a singular interaction.
 __device__ __forceinline__ bool point_mass_factor(double d2, double m, double g, double soft2, double &f) {
   const double r2 = __dadd_rn(d2, soft2);
-  const double inv = __ddiv_rn(1.0, __dsqrt_rn(r2));
+  const double inv = __drcp_rn(__dsqrt_rn(r2));
   const double inv3 = __dmul_rn(__dmul_rn(inv, inv), inv);
   f = __dmul_rn(__dmul_rn(g, m), inv3);
   return !(r2 <= 0.0);

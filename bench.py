@@ -333,7 +333,7 @@ def run_nbb(args, rank, world, local):
 BUILD_BYTES_PER_PARTICLE = (152 + 32 + 4 * 16     # kick-drift + box (+ position records), encode, 4 sort passes
                             + 20 + 76 + 32 + 1)   # groups, Morton gather, leaf mass, target-group scan
 BUILD_BYTES_PER_GROUP = 16 + 24 + 20 + 124        # group arrays, level spans, cell ranks, leaf records
-BUILD_BYTES_PER_OCTREE_NODE = 32 + 48             # cell entries, read once as a child
+BUILD_BYTES_PER_OCTREE_NODE = 32 + 48 + 12        # cell entries, read once as a child, arrival counter
 BUILD_BYTES_PER_INTERNAL_NODE = 160               # level pass: entries, LevelNode, MixedNode, child list
 
 

@@ -351,14 +351,14 @@ int nbb_measure_fma_tflops(int precision, double *tflops);
  * loading, CUDA's default, it is placed when the module loads, at the first
  * call of the library on that device).  x, y, z, keys and idx are device
  * pointers of n elements; larger n is rejected with
- * NBB_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) and should come before any stream
- * capture; the address is kept per device number, so after a
- * cudaDeviceReset, or from another context on the same device, the process
- * must not call this entry point again.  Every call shares the array: calls
- * that overlap on the GPU (other
- * streams, other threads) race and give wrong results.  The call synchronises
- * the given stream before it returns.  Its errors are reported by
+ * NBB_ERR_INVALID_ARGUMENT.  Every call looks up the array's device address
+ * in the current context (cudaGetSymbolAddress; nothing is cached, so a reset
+ * device or another context is served by its own copy).  The call reads its
+ * error word back and synchronises the given stream before it returns, so it
+ * cannot be captured in a CUDA graph: on a capturing stream it returns
+ * NBB_ERR_INVALID_ARGUMENT without touching the capture.  Every call shares
+ * the array: calls that overlap on the GPU (other streams, other threads)
+ * race and give wrong results.  Its errors are reported by
  * nbb_noalloc_last_error_message(). */
 #define NBB_NOALLOC_MAX_PARTICLES (1 << 18)
 int nbb_morton_sort_noalloc(const double *x, const double *y, const double *z,

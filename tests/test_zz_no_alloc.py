@@ -119,3 +119,25 @@ def test_noalloc_sort_takes_no_device_memory(nbb_mod):
     free1, _ = torch.cuda.mem_get_info(dev)
     assert st == 0, text
     assert free1 == free0
+
+
+def test_noalloc_sort_refuses_stream_capture(nbb_mod):
+    # the call reads its error word back and synchronises, which a capture
+    # forbids: on a capturing stream it returns NBB_ERR_INVALID_ARGUMENT and
+    # leaves the capture intact
+    import torch
+
+    fn, msg = _bind(nbb_mod.load())
+    dev = torch.device("cuda:0")
+    x = torch.zeros(1000, dtype=torch.float64, device=dev)
+    keys = torch.zeros(1000, dtype=torch.int32, device=dev)
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream(dev)
+    with torch.cuda.graph(g, stream=s):
+        st = fn(C.c_void_p(x.data_ptr()), C.c_void_p(x.data_ptr()), C.c_void_p(x.data_ptr()), 1000,
+                C.c_void_p(keys.data_ptr()), C.c_void_p(keys.data_ptr()), C.c_void_p(s.cuda_stream))
+        keys.add_(1)
+    assert st == 1 and "captured" in msg().decode()
+    g.replay()
+    torch.cuda.synchronize()
+    assert int(keys.sum()) == 1000
