@@ -186,7 +186,25 @@ constexpr int kMixedWarps = NBB_MIXED_WARPS;
 constexpr int kWalkPop = 64;     // nodes per round: two per lane
 constexpr int kStackCap = 1024;  // shared-memory part of a warp's stack
 constexpr int kSpill = 512;      // entries moved to / from the global extension at once
-constexpr int kListCap = 192;    // < 32 left over + 64 cells + up to 96 leaf particles
+// Entries per evaluated batch of the force walk: the list is evaluated when it
+// holds this many, so each batch's set-up and compensated addition are paid
+// once per kEvalBatch entries.  The walks that track sources (zero softening,
+// the adjoint) keep 32-entry batches and the smaller list, whose shared
+// memory keeps 10 blocks per SM.
+#ifndef NBB_EVAL_BATCH
+#define NBB_EVAL_BATCH 64
+#endif
+constexpr int kEvalBatch = NBB_EVAL_BATCH;
+static_assert(kEvalBatch % 32 == 0 && kEvalBatch >= 32 && kEvalBatch <= 128, "batch of whole warps");
+template <bool kTrackSource>
+__host__ __device__ constexpr int batch_of() {
+  return kTrackSource ? 32 : kEvalBatch;
+}
+// list capacity: < batch left over + 64 cells + up to 96 leaf particles
+template <bool kTrackSource>
+__host__ __device__ constexpr int list_cap_of() {
+  return batch_of<kTrackSource>() + 160;
+}
 
 // The interaction list keeps entries in pairs so that packed two-wide FP32
 // instructions (sm_100's FADD2 / FMUL2 / FFMA2) evaluate two entries at once
@@ -210,9 +228,9 @@ struct MixedShared {
   double gbox[kMixedWarps][9];  // group box lo (3), hi (3), centre (3)
   float ghalf[kMixedWarps][4];  // group box half extents, rounded up to FP32
   int stack[kMixedWarps][kStackCap];
-  float4 la[kMixedWarps][kListCap / 2];
-  float4 lb[kMixedWarps][kListCap / 2];
-  int src[kMixedWarps][kTrackSource ? kListCap : 1];
+  float4 la[kMixedWarps][list_cap_of<kTrackSource>() / 2];
+  float4 lb[kMixedWarps][list_cap_of<kTrackSource>() / 2];
+  int src[kMixedWarps][kTrackSource ? list_cap_of<kTrackSource>() : 1];
 };
 
 // Hardware approximate reciprocal square root (MUFU), subnormal inputs and
@@ -438,32 +456,36 @@ __device__ bool vjp_entries(const PairList &list, const int *src, int count, int
 template <bool kTrackSource, int kTPL, bool kVjp>
 __device__ __forceinline__ void flush_full(const PairList &list, int *src, int &ls, LaneTargets<kTPL> &lt_,
                                            LaneVjp &vj, float2 eps2, int nq, float g, const AdjointBuffers &ab) {
+  constexpr int kBatch = batch_of<kTrackSource>();
   const int lane = threadIdx.x & 31;
   int done = 0;
-  while (ls - done >= 32) {
+  while (ls - done >= kBatch) {
     const PairList part{list.a + done / 2, list.b + done / 2};
     bool sg;
     if constexpr (kVjp)
-      sg = vjp_entries(part, src + done, 32, lt_.s[0], lt_.valid[0], lt_.ntx[0].x, lt_.nty[0].x, lt_.ntz[0].x, vj,
-                       eps2.x, g, ab);
+      sg = vjp_entries(part, src + done, kBatch, lt_.s[0], lt_.valid[0], lt_.ntx[0].x, lt_.nty[0].x, lt_.ntz[0].x,
+                       vj, eps2.x, g, ab);
     else
-      sg = eval_slots<kTrackSource, kTPL>(part, src + (kTrackSource ? done : 0), 32, nq, lt_, eps2);
+      sg = eval_slots<kTrackSource, kTPL>(part, src + (kTrackSource ? done : 0), kBatch, nq, lt_, eps2);
 #pragma unroll
     for (int q = 0; q < kTPL; ++q)
       if (lt_.valid[q]) {
-        lt_.inter += 32;
+        lt_.inter += kBatch;
         lt_.singular |= sg;
       }
-    done += 32;
+    done += kBatch;
   }
   if (done) {
     __syncwarp();
+    // fewer than kBatch entries left; the sources start at done >= kBatch,
+    // past the destinations
     const int rest = ls - done;
-    if (lane < (rest + 1) / 2) {
-      list.a[lane] = list.a[done / 2 + lane];
-      list.b[lane] = list.b[done / 2 + lane];
+    for (int i = lane; i < (rest + 1) / 2; i += 32) {
+      list.a[i] = list.a[done / 2 + i];
+      list.b[i] = list.b[done / 2 + i];
     }
-    if (kTrackSource && lane < rest) src[lane] = src[done + lane];
+    if (kTrackSource)
+      for (int i = lane; i < rest; i += 32) src[i] = src[done + i];
     ls = rest;
     __syncwarp();
   }
@@ -834,7 +856,7 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
         ltotal = __shfl_sync(kFull, linc, 31);
         lexcl = linc - lc0 - lc1;
       }
-      if (ls + ltotal <= kListCap) {
+      if (ls + ltotal <= list_cap_of<kTrackSource>()) {
         const int base = ls + lexcl;
         double4 q0 = make_double4(0.0, 0.0, 0.0, 0.0), q1 = q0;
         if (lc0 > 0) q0 = ws.pm4[m0.y];
