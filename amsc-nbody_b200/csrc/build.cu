@@ -1587,16 +1587,19 @@ __global__ void __launch_bounds__(32 * kLevelOrderChannels) lo_tile_scan_kernel(
   }
 }
 
-// One cell's records from its mass sums: the LevelNode its parent reads, the
-// geometry from the key prefix (octree_geometry.cu:56-102) and the traversal
-// records at the preorder index (as layout_kernel writes them).  The child
-// list is the caller's.  Neither walk applies the acceptance test to an
-// occupied leaf (its particles are summed), so a leaf gets no geometry and no
-// acceptance radius.  Returns false on an invalid system id.
-template <int kRecords>
-__device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double theta, int b, int pre, int skip,
-                                        int pf, int pe, bool leaf, int nk, double tm, double wx, double wy,
-                                        double wz, unsigned long long key) {
+// A finished cell of the upward pass whose traversal records are still to
+// be written: its mass and centre of mass and what the records need.
+struct LoCell {
+  double4 a;  // centre of mass, mass
+  unsigned long long key;
+  int level, pre, skip, pf, pe, nk;
+  bool leaf;
+};
+
+// One cell's mass and centre of mass from its sums, and the LevelNode its
+// parent reads (the only record another thread of the upward pass needs).
+__device__ __forceinline__ void lo_emit_node(const Workspace &ws, int b, double tm, double wx, double wy, double wz,
+                                             LoCell &c) {
   double comx = 0.0, comy = 0.0, comz = 0.0;
   if (tm > 0.0) {
     const double inv = __drcp_rn(tm);
@@ -1604,22 +1607,35 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
     comy = __dmul_rn(wy, inv);
     comz = __dmul_rn(wz, inv);
   }
-  const double4 a = make_double4(comx, comy, comz, tm);
+  c.a = make_double4(comx, comy, comz, tm);
   LevelNode rec;
-  rec.a = a;
-  rec.pre = pre;
-  rec.np = pe - pf;
-  rec.first = pf;
-  rec.leaf = leaf ? 1 : 0;
+  rec.a = c.a;
+  rec.pre = c.pre;
+  rec.np = c.pe - c.pf;
+  rec.first = c.pf;
+  rec.leaf = c.leaf ? 1 : 0;
   ws.lo_node[b] = rec;
+}
+
+// A finished cell's geometry from the key prefix (octree_geometry.cu:56-102)
+// and its traversal records at the preorder index (as layout_kernel writes
+// them).  The child list is the caller's.  Neither walk applies the
+// acceptance test to an occupied leaf (its particles are summed), so a leaf
+// gets no geometry and no acceptance radius.  Returns false on an invalid
+// system id.
+template <int kRecords>
+__device__ __forceinline__ bool lo_emit_records(const Workspace &ws, double theta, const LoCell &c) {
+  const int level = c.level, pre = c.pre;
+  const bool leaf = c.leaf;
+  const double4 a = c.a;
   double cx = 0.0, cy = 0.0, cz = 0.0, h = 0.0;
   if (level >= ws.sys_levels) {
-    const unsigned long long sys = key >> kSpatialBits;
+    const unsigned long long sys = c.key >> kSpatialBits;
     if (sys >= (unsigned long long)ws.n_systems) return false;
     if (level == ws.sys_levels) ws.root_pre[sys] = pre;
   }
   if (level >= ws.sys_levels && !leaf) {
-    const unsigned long long sys = key >> kSpatialBits;
+    const unsigned long long sys = c.key >> kSpatialBits;
     const double *box = ws.sys_box + 4 * (size_t)sys;
     cx = box[0];
     cy = box[1];
@@ -1627,7 +1643,7 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
     h = __dmul_rn(box[3], 0.5);
     const int kb = ws.key_bits;
     for (int d = ws.sys_levels + 1; d <= level; ++d) {
-      const int oct = (int)((key >> (kb - d * kDims)) & 7ull);
+      const int oct = (int)((c.key >> (kb - d * kDims)) & 7ull);
       const double ch = __dmul_rn(h, 0.5);
       cx = __dadd_rn(cx, (oct & 4) ? ch : -ch);
       cy = __dadd_rn(cy, (oct & 2) ? ch : -ch);
@@ -1639,7 +1655,7 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
   double crit = 0.0, c2 = 0.0, cm = 0.0;
   if (!leaf) {
     const double side = __dmul_rn(2.0, h);
-    const double ox = __dsub_rn(comx, cx), oy = __dsub_rn(comy, cy), oz = __dsub_rn(comz, cz);
+    const double ox = __dsub_rn(a.x, cx), oy = __dsub_rn(a.y, cy), oz = __dsub_rn(a.z, cz);
     const double o2 = __fma_rn(oz, oz, __fma_rn(oy, oy, __dmul_rn(ox, ox)));
     crit = (theta > 0.0) ? __dadd_rn(__ddiv_rn(side, theta), __dsqrt_rn(o2)) : INFINITY;
     c2 = __dmul_rn(crit, crit);
@@ -1652,15 +1668,15 @@ __device__ __forceinline__ bool lo_emit(const Workspace &ws, int level, double t
       ws.node_b[pre] = make_double4(cx, cy, cz, h);
       ws.node_c[pre] = make_double4(crit, c2 * (1.0 - 0x1p-44), c2 * (1.0 + 0x1p-44), cm * cm);
     }
-    ws.node_meta[pre] = make_int4(skip, leaf ? pf : -1, leaf ? pe - pf : 0, nk);
+    ws.node_meta[pre] = make_int4(c.skip, leaf ? c.pf : -1, leaf ? c.pe - c.pf : 0, c.nk);
   }
   if (kRecords & kRecordsMixed) {
     MixedNode mrec;
     mrec.a = a;
     mrec.cr2 = leaf ? 0.f : __double2float_ru(cm * cm * (1.0 + 0x1p-18));
-    mrec.first = leaf ? pf : -1;
-    mrec.count = leaf ? pe - pf : 0;
-    mrec.nchild = nk;
+    mrec.first = leaf ? c.pf : -1;
+    mrec.count = leaf ? c.pe - c.pf : 0;
+    mrec.nchild = c.nk;
     ws.node_m[pre] = mrec;
   }
   return true;
@@ -1859,6 +1875,48 @@ __device__ __forceinline__ bool lo_whole_group(const Workspace &ws, int level, i
   return !virt && np <= ws.group_max && compact;
 }
 
+// The occupied leaf of group g: mass and centre of mass of the group's
+// particles in sorted order (octree_physics.cu:95-154), its LevelNode and its
+// target-group marks; the traversal records (at preorder index S(g) - 1, no
+// child list: neither walk reads one for an occupied leaf) are the caller's
+// (lo_emit_records with c).  Returns the leaf's level-order index, or false
+// on inconsistent input.
+__device__ __forceinline__ bool lo_leaf_cell(const Workspace &ws, int g, int M, int &bleaf, LoCell &c) {
+  DevScalars *sc = ws.sc;
+  const int2 lf = ws.lo_gleaf[g];
+  const int pf = ws.gfirst[g], pe = ws.glast[g] + 1;
+  c.key = ws.ukey[g];
+  c.level = (ws.gspan[g] >> 8) & 255;
+  bleaf = lf.x;
+  c.skip = lf.y;
+  c.pre = c.skip - 1;
+  c.pf = pf;
+  c.pe = pe;
+  c.nk = 0;
+  c.leaf = true;
+  if (bleaf < 0 || bleaf >= M || c.pre < 0 || c.pre >= M || pf < 0 || pe <= pf || pe > ws.n || c.level < 1 ||
+      c.level > ws.max_level) {
+    record_error(sc, kStageLayout, 1);
+    return false;
+  }
+  double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  for (int i = pf; i < pe; ++i) {
+    const double4 q = ws.pm4[i];
+    tm = __dadd_rn(tm, q.w);
+    wx = __fma_rn(q.w, q.x, wx);
+    wy = __fma_rn(q.w, q.y, wy);
+    wz = __fma_rn(q.w, q.z, wz);
+  }
+  lo_emit_node(ws, bleaf, tm, wx, wy, wz, c);
+  const int np = pe - pf;
+  if (lo_whole_group(ws, c.level, np, true)) {
+    if (c.level == ws.sys_levels) ws.tflag[pf] = 1;
+  } else {
+    for (int k = 0; k < np; k += ws.group_max) ws.tflag[pf + k] = 1;
+  }
+  return true;
+}
+
 // A child's LevelNode, written earlier in the same kernel by another thread
 // of the upward pass: read from L2 (ld.global.cg), never from a stale L1 line.
 __device__ __forceinline__ LevelNode ld_level_node_cg(const LevelNode *p) {
@@ -1874,53 +1932,14 @@ __device__ __forceinline__ LevelNode ld_level_node_cg(const LevelNode *p) {
   return r;
 }
 
-// The occupied leaf of group g: mass and centre of mass of the group's
-// particles in sorted order (octree_physics.cu:95-154), the leaf's records at
-// preorder index S(g) - 1 (no child list: neither walk reads one for an
-// occupied leaf), and its target-group marks.  Returns the leaf's level-order
-// index and level, or false on inconsistent input.
-template <int kRecords>
-__device__ __forceinline__ bool lo_leaf_cell(const Workspace &ws, double theta, int g, int M, int &bleaf, int &lam) {
-  DevScalars *sc = ws.sc;
-  const int2 lf = ws.lo_gleaf[g];
-  const int pf = ws.gfirst[g], pe = ws.glast[g] + 1;
-  const unsigned long long key = ws.ukey[g];
-  lam = (ws.gspan[g] >> 8) & 255;
-  bleaf = lf.x;
-  const int skip = lf.y, pre = skip - 1;
-  if (bleaf < 0 || bleaf >= M || pre < 0 || pre >= M || pf < 0 || pe <= pf || pe > ws.n || lam < 1 ||
-      lam > ws.max_level) {
-    record_error(sc, kStageLayout, 1);
-    return false;
-  }
-  double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
-  for (int i = pf; i < pe; ++i) {
-    const double4 q = ws.pm4[i];
-    tm = __dadd_rn(tm, q.w);
-    wx = __fma_rn(q.w, q.x, wx);
-    wy = __fma_rn(q.w, q.y, wy);
-    wz = __fma_rn(q.w, q.z, wz);
-  }
-  if (!lo_emit<kRecords>(ws, lam, theta, bleaf, pre, skip, pf, pe, true, 0, tm, wx, wy, wz, key)) {
-    record_error(sc, kStageGeometry, 2);
-    return false;
-  }
-  const int np = pe - pf;
-  if (lo_whole_group(ws, lam, np, true)) {
-    if (lam == ws.sys_levels) ws.tflag[pf] = 1;
-  } else {
-    for (int k = 0; k < np; k += ws.group_max) ws.tflag[pf + k] = 1;
-  }
-  return true;
-}
-
 // One internal cell b of a level (children in the next level's range
-// [hi, end)): mass and centre of mass from the children's records in octant
-// order (octree_physics.cu:156-245), target-group marks, then the records.
-// Returns false on inconsistent input.
-template <int kRecords>
-__device__ __forceinline__ bool lo_level_cell(const Workspace &ws, int level, double theta, int b, int hi, int end,
-                                              int M, const int4 &f, const int4 &q, int next_first_child) {
+// [hi, end); f, q its lo_first and lo_last entries): mass and centre of mass
+// from the children's records in octant order (octree_physics.cu:156-245),
+// the child list, the target-group marks and its LevelNode; the traversal
+// records are the caller's (lo_emit_records with c).  Returns false on
+// inconsistent input.
+__device__ __forceinline__ bool lo_level_cell(const Workspace &ws, int level, int b, int hi, int end, int M,
+                                              const int4 &f, const int4 &q, int next_first_child, LoCell &c) {
   DevScalars *sc = ws.sc;
   const int c0 = f.y;
   const int c1 = (b + 1 < hi) ? next_first_child : end;
@@ -1931,6 +1950,14 @@ __device__ __forceinline__ bool lo_level_cell(const Workspace &ws, int level, do
     return false;
   }
   const int nk = c1 - c0;
+  c.level = level;
+  c.pre = pre;
+  c.skip = skip;
+  c.pf = pf;
+  c.pe = pe;
+  c.nk = nk;
+  c.leaf = false;
+  c.key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
   // children in visit order: octant 7 -> 0, the children in descending key order
   int *kids = ws.node_kids + (size_t)pre * 8;
   // target groups (group_mark_kernel's rule): a whole system that is one
@@ -1969,11 +1996,7 @@ __device__ __forceinline__ bool lo_level_cell(const Workspace &ws, int level, do
     }
   }
   for (int j = nk; j < 8; ++j) kids[j] = -1;
-  const unsigned long long key = (unsigned long long)(unsigned)q.z | ((unsigned long long)(unsigned)q.w << 32);
-  if (!lo_emit<kRecords>(ws, level, theta, b, pre, skip, pf, pe, false, nk, tm, wx, wy, wz, key)) {
-    record_error(sc, kStageGeometry, 2);
-    return false;
-  }
+  lo_emit_node(ws, b, tm, wx, wy, wz, c);
   return true;
 }
 
@@ -2005,14 +2028,23 @@ __device__ __forceinline__ bool lo_arrive_last(const Workspace &ws, int c, int p
 // The whole upward pass in one launch, with arrival counters instead of one
 // launch per level: a thread finishes the leaf of group g, then climbs.  At
 // each parent it counts itself in (lo_arrive_last: an acquire-release atomic
-// publishes the child's records); the child that arrives last finishes the
+// publishes the child's LevelNode); the child that arrives last finishes the
 // parent from its children's records and climbs on, the others stop.  Every
 // cell is finished exactly once, after all of its children, with the same
 // arithmetic in the same child order as a level-by-level pass.  No thread
 // ever waits: a climb ends at the root, at a parent that other children
-// still owe, or at the first inconsistency.
+// still owe, or at the first inconsistency.  What keeps the climb short: a
+// cell's traversal records (geometry, acceptance radius, the scattered
+// writes at the preorder index) are written after its arrival, not before;
+// the parent's entries are read before the arrival; and a block is one warp
+// (32 resident per SM, 64 registers), so a warp whose lanes climb far holds
+// no other warp's slot.  Measured at 2^20 particles (kernel time, cold):
+// 174 us before these three changes, 152 us after (blocks of 64: 156 us,
+// of 256: 170 us; one-warp blocks at 78 registers, 26 per SM: 163 us).
+constexpr int kUpsweepBlock = 32;
+
 template <int kRecords>
-__global__ void __launch_bounds__(kBlock, 4) lo_upsweep_kernel(Workspace ws, double theta) {
+__global__ void __launch_bounds__(kUpsweepBlock, 32) lo_upsweep_kernel(Workspace ws, double theta) {
   __shared__ int s_g, s_m;
   __shared__ int s_base[kMaxLevels + 2];
   DevScalars *sc = ws.sc;
@@ -2029,32 +2061,39 @@ __global__ void __launch_bounds__(kBlock, 4) lo_upsweep_kernel(Workspace ws, dou
     return;
   }
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
-    int cell, level;
-    if (!lo_leaf_cell<kRecords>(ws, theta, g, M, cell, level)) continue;
+    int cell;
+    LoCell c;
+    if (!lo_leaf_cell(ws, g, M, cell, c)) continue;
     // the cell's parent and its neighbours' (which children are first and last)
+    int level = c.level;
     int p = ws.lo_first[cell].w;
     int pl = cell > s_base[level] ? ws.lo_first[cell - 1].w : -1;
     int pr = cell + 1 < s_base[level + 1] ? ws.lo_first[cell + 1].w : -1;
-    while (level > 0) {
+    while (true) {
+      if (level == 0) {
+        if (!lo_emit_records<kRecords>(ws, theta, c)) record_error(sc, kStageGeometry, 2);
+        break;
+      }
       const int lv = level - 1;
       const int lo = s_base[lv], hi = s_base[lv + 1], end = s_base[lv + 2];
       if (p < lo || p >= hi) {
         record_error(sc, kStageLayout, 1);
         break;
       }
-      bool bad;
-      const bool last = lo_arrive_last(ws, cell, p, pl, pr, bad);
-      if (!last) {
-        if (bad) record_error(sc, kStageLayout, 1);
-        break;
-      }
       // the parent's entries, its successor's first child and the parents of
-      // its neighbours, in one round trip
+      // its neighbours: read-only here, loaded before the arrival
       const int4 f = ws.lo_first[p];
       const int4 q = ws.lo_last[p];
       const int4 fr = (p + 1 < hi) ? ws.lo_first[p + 1] : make_int4(0, end, 0, -1);
       const int npl = p > lo ? ws.lo_first[p - 1].w : -1;
-      if (!lo_level_cell<kRecords>(ws, lv, theta, p, hi, end, M, f, q, fr.y)) break;
+      bool bad;
+      const bool last = lo_arrive_last(ws, cell, p, pl, pr, bad);
+      if (!lo_emit_records<kRecords>(ws, theta, c)) record_error(sc, kStageGeometry, 2);
+      if (!last) {
+        if (bad) record_error(sc, kStageLayout, 1);
+        break;
+      }
+      if (!lo_level_cell(ws, lv, p, hi, end, M, f, q, fr.y, c)) break;
       cell = p;
       level = lv;
       p = f.w;
@@ -2360,15 +2399,16 @@ cudaError_t launch_level_order_tree(Workspace &ws, double theta, cudaStream_t s)
   else
     lo_rank_kernel<kRecordsFp64 | kRecordsMixed><<<ws.scan_tiles_n, kScanThreads, 0, s>>>(ws, theta);
   // leaves and every internal cell in one launch (arrival counters), one
-  // thread per group (a resident grid taking groups grid-stride measured
-  // slower: 267 against 174 us at 2^20 particles)
-  const int leaf_grid = (ws.n + kBlock - 1) / kBlock > 0 ? (ws.n + kBlock - 1) / kBlock : 1;
+  // thread per group in one-warp blocks (a resident grid taking groups
+  // grid-stride measured slower: 267 against 174 us at 2^20 particles)
+  const int want = (ws.n + kUpsweepBlock - 1) / kUpsweepBlock;
+  const int up_grid = want > 0 ? want : 1;
   if (ws.records == kRecordsMixed)
-    lo_upsweep_kernel<kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+    lo_upsweep_kernel<kRecordsMixed><<<up_grid, kUpsweepBlock, 0, s>>>(ws, theta);
   else if (ws.records == kRecordsFp64)
-    lo_upsweep_kernel<kRecordsFp64><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+    lo_upsweep_kernel<kRecordsFp64><<<up_grid, kUpsweepBlock, 0, s>>>(ws, theta);
   else
-    lo_upsweep_kernel<kRecordsFp64 | kRecordsMixed><<<leaf_grid, kBlock, 0, s>>>(ws, theta);
+    lo_upsweep_kernel<kRecordsFp64 | kRecordsMixed><<<up_grid, kUpsweepBlock, 0, s>>>(ws, theta);
   if (ws.top && (ws.records & kRecordsMixed) && ws.n_systems == 1) {
     lo_top_kernel<<<1, 128, 0, s>>>(ws);
     count_launches(1);
