@@ -120,6 +120,7 @@ const char *device_message(int stage, int code) {
         case 6: return "Singular gravitational interaction; use positive softening";
         case 7: return "Occupied octree leaf unexpectedly has children";
         case 8: return "Octree node has invalid geometry";
+        case 9: return "Mixed-precision traversal ran out of stack space; nodes were accepted untested";
         default: return "Unknown Barnes-Hut traversal error";
       }
     case kStageLayout:

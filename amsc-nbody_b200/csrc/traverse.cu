@@ -966,7 +966,12 @@ __global__ void __launch_bounds__(kMixedWarps * 32,
   if (lane == 0) {
     atomicAdd(&sc->interactions, (unsigned long long)inter_total);
     atomicAdd(&sc->mac_tests, (unsigned long long)tests);
-    if (ov) atomicAdd(&sc->stack_overflow, ov);
+    if (ov) {
+      // the extension is sized for any walk, so this is a broken invariant:
+      // the accepted nodes skipped their acceptance test, and the call fails
+      atomicAdd(&sc->stack_overflow, ov);
+      record_error(sc, kStageTraversal, 9);
+    }
   }
 }
 

@@ -163,8 +163,10 @@ typedef struct {
   int64_t mac_tests;    /* acceptance tests evaluated */
   int group_size;       /* MIXED: warp target group size in use (32, 64 or 128) */
   int64_t stack_overflow; /* MIXED: nodes accepted because the walk's stack was
-                             full (their children would not fit); 0 in a walk
-                             that applied the acceptance test everywhere */
+                             full (their children would not fit).  The stack's
+                             global extension is sized for any walk, so this is
+                             0; a nonzero count also fails the call or step with
+                             NBB_ERR_DEVICE */
   int cache_depth;      /* MIXED: tree levels below the root the walk stages in
                            shared memory per block (0, 1 or 2; autotuned) */
 } nbb_stats;
