@@ -186,6 +186,10 @@ constexpr int kMixedWarps = NBB_MIXED_WARPS;
 constexpr int kWalkPop = 64;     // nodes per round: two per lane
 constexpr int kStackCap = 1024;  // shared-memory part of a warp's stack
 constexpr int kSpill = 512;      // entries moved to / from the global extension at once
+// A spill starts above kStackCap - 7 kWalkPop entries and moves the bottom
+// kSpill of them, so that threshold must hold at least kSpill entries (and
+// the moved-down rest must end below kSpill, where the sources start).
+static_assert(kStackCap - 7 * kWalkPop >= kSpill && kStackCap <= 2 * kSpill, "stack spill bounds");
 // Entries per evaluated batch of the force walk: the list is evaluated when it
 // holds this many, so each batch's set-up and compensated addition are paid
 // once per kEvalBatch entries.  The walks that track sources (zero softening,
